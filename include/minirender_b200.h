@@ -1,0 +1,404 @@
+/*
+ * minirender_b200.h — C ABI of the B200 offline path tracer.
+ *
+ * This is the drop-in boundary for MiniRender's CPU offline render call. The reference has no
+ * FFI: its callers link the C++ classes `PathTracer` (include/minirender/render/path_tracer.hpp)
+ * and `RenderSession` (include/minirender/render/render_session.hpp). Every entry point below
+ * replaces one of those calls; the citation beside it names the reference interface
+ * (file:line inside the MiniRender source tree).
+ *
+ * Conventions
+ *  - Plain C: pointers, sizes and POD structs. No C++ or torch types cross the boundary.
+ *  - Every call returns an `mr_status`. C++ exceptions of the reference map onto status codes
+ *    (std::invalid_argument -> MR_INVALID_ARGUMENT, std::overflow_error -> MR_OVERFLOW, ...);
+ *    `mr_last_error` returns the message of the calling thread's last failure.
+ *  - Host pointers are host memory unless the name says `device`.
+ *  - All device arithmetic is FP32. Scene inputs keep the reference's types (float meshes and
+ *    matrices, double medium coefficients), so the same descriptor also feeds the CPU oracle.
+ *  - The library never falls back to the CPU: without a usable CUDA device every compute entry
+ *    point returns MR_CUDA_ERROR.
+ */
+#ifndef MINIRENDER_B200_H
+#define MINIRENDER_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MR_ABI_VERSION 1u
+
+typedef enum mr_status {
+    MR_OK               = 0,
+    MR_INVALID_ARGUMENT = 1, /* std::invalid_argument */
+    MR_OUT_OF_RANGE     = 2, /* std::out_of_range */
+    MR_OVERFLOW         = 3, /* std::overflow_error: radiance above FLT_MAX */
+    MR_RUNTIME_ERROR    = 4, /* std::runtime_error: nonfinite or negative path contribution */
+    MR_CANCELLED        = 5, /* OperationCancelled */
+    MR_LOGIC_ERROR      = 6, /* std::logic_error: session still active */
+    MR_LENGTH_ERROR     = 7, /* std::length_error: index range exceeded */
+    MR_CUDA_ERROR       = 8, /* CUDA runtime failure or no device */
+    MR_OUT_OF_MEMORY    = 9, /* device allocation failed or HBM budget exceeded */
+    MR_TIMEOUT          = 10 /* a bounded device or host wait gave up */
+} mr_status;
+
+/* MaterialKind (include/minirender/scene/scene.hpp:106). cloth and subsurface are rejected. */
+typedef enum mr_material_kind {
+    MR_MATERIAL_DIFFUSE    = 0,
+    MR_MATERIAL_CONDUCTOR  = 1,
+    MR_MATERIAL_MIRROR     = 2,
+    MR_MATERIAL_DIELECTRIC = 3,
+    MR_MATERIAL_CLOTH      = 4,
+    MR_MATERIAL_SUBSURFACE = 5
+} mr_material_kind;
+
+/* SamplingMode (include/minirender/render/path_tracer.hpp:13). */
+typedef enum mr_sampling_mode {
+    MR_SAMPLING_BSDF  = 0,
+    MR_SAMPLING_LIGHT = 1,
+    MR_SAMPLING_MIS   = 2
+} mr_sampling_mode;
+
+/* RenderState (include/minirender/render/render_session.hpp:12-23). */
+typedef enum mr_render_state {
+    MR_STATE_IDLE       = 0,
+    MR_STATE_PREPARING  = 1,
+    MR_STATE_RUNNING    = 2,
+    MR_STATE_PAUSING    = 3,
+    MR_STATE_PAUSED     = 4,
+    MR_STATE_FINALIZING = 5,
+    MR_STATE_CANCELLING = 6,
+    MR_STATE_CANCELLED  = 7,
+    MR_STATE_COMPLETED  = 8,
+    MR_STATE_FAILED     = 9
+} mr_render_state;
+
+/* Camera (include/minirender/scene/scene.hpp:85-104). */
+typedef struct mr_camera {
+    float position[3];
+    float target[3];
+    float up[3];
+    float vertical_fov_degrees;
+    float near_plane;
+    float far_plane;
+    float aperture_radius;
+    float focus_distance;
+} mr_camera;
+
+/* Material (include/minirender/scene/scene.hpp:113-136), the fields the offline path reads. */
+typedef struct mr_material {
+    uint32_t kind; /* mr_material_kind */
+    float    base_color[3];
+    float    emission[3];
+    float    roughness;
+    float    ior;
+    uint32_t double_sided;
+} mr_material;
+
+/* MeshCorner (include/minirender/scene/scene.hpp:33-37): 24 bytes. */
+typedef struct mr_mesh_corner {
+    uint32_t position;
+    float    normal[3];
+    float    uv[2];
+} mr_mesh_corner;
+
+/* MeshData (include/minirender/scene/scene.hpp:45-50): positions and 3 corners per triangle. */
+typedef struct mr_mesh {
+    const float*          positions; /* 3 * position_count */
+    uint32_t              position_count;
+    const mr_mesh_corner* corners; /* 3 * triangle_count */
+    uint32_t              triangle_count;
+} mr_mesh;
+
+/* RenderInstance (include/minirender/scene/scene.hpp:201-209). Matrices are column-major
+ * (glm layout): object_to_world[4*c + r], normal_to_world[3*c + r]. */
+typedef struct mr_instance {
+    uint32_t mesh;
+    uint32_t material;
+    float    object_to_world[16];
+    float    normal_to_world[9];
+} mr_instance;
+
+/* DirectionalLight (include/minirender/scene/scene.hpp:170-175). */
+typedef struct mr_directional_light {
+    float direction[3];
+    float color[3];
+    float intensity;
+} mr_directional_light;
+
+/* MediumRegion + HomogeneousMedium (include/minirender/scene/medium.hpp:14-41). */
+typedef struct mr_medium_region {
+    double   minimum[3];
+    double   maximum[3];
+    double   absorption[3];
+    double   scattering[3];
+    double   anisotropy;
+    uint32_t enabled;
+} mr_medium_region;
+
+/* SceneSnapshot (include/minirender/scene/scene.hpp:220-230) without textures. */
+typedef struct mr_scene_desc {
+    mr_camera                   camera;
+    float                       environment[3];
+    const mr_mesh*              meshes;
+    uint32_t                    mesh_count;
+    const mr_material*          materials;
+    uint32_t                    material_count;
+    const mr_instance*          instances;
+    uint32_t                    instance_count;
+    const mr_directional_light* directional_lights;
+    uint32_t                    directional_light_count;
+    const mr_medium_region*     media;
+    uint32_t                    medium_count;
+} mr_scene_desc;
+
+/* SceneBvh::Node (include/minirender/render/bvh.hpp:81-86), the reference's flat node layout.
+ * Leaf: count > 0 and [first, first+count) indexes `order`. Interior: count == 0, `first` is
+ * the left child and `right` the right child. Primitive ids enumerate instances in order and
+ * their triangles in order, as in SceneBvh's constructor (src/render/bvh.cpp:163-199). */
+typedef struct mr_bvh_node {
+    float    minimum[3];
+    float    maximum[3];
+    uint32_t first;
+    uint32_t right;
+    uint32_t count;
+} mr_bvh_node;
+
+typedef struct mr_bvh_desc {
+    const mr_bvh_node* nodes;
+    uint32_t           node_count;
+    const uint32_t*    order;
+    uint32_t           primitive_count;
+} mr_bvh_desc;
+
+/* IntegratorSettings (include/minirender/render/path_tracer.hpp:21-35), path tracing only. */
+typedef struct mr_integrator_settings {
+    uint32_t mode; /* mr_sampling_mode */
+    uint32_t maximum_depth;
+    uint32_t russian_roulette;
+    uint32_t roulette_depth;
+} mr_integrator_settings;
+
+/* RenderSettings (include/minirender/render/path_tracer.hpp:38-49). */
+typedef struct mr_render_settings {
+    uint64_t width;
+    uint64_t height;
+    uint32_t samples_per_pixel;
+    uint64_t seed;
+} mr_render_settings;
+
+/* SessionSettings (include/minirender/render/render_session.hpp:30-38). On the GPU `threads` is
+ * accepted for validation only; tile_size and batch_samples keep their meaning: one committed
+ * unit of work is a tile_size^2 block of pixels advanced by batch_samples samples. */
+typedef struct mr_session_settings {
+    uint32_t threads;
+    uint32_t tile_size;
+    uint32_t batch_samples;
+} mr_session_settings;
+
+/* TraceStatistics (include/minirender/render/bvh.hpp:37-40). */
+typedef struct mr_trace_statistics {
+    uint64_t bounds_tests;
+    uint64_t triangle_tests;
+} mr_trace_statistics;
+
+/* PathStatistics (include/minirender/render/path_tracer.hpp:52-68). */
+typedef struct mr_path_statistics {
+    mr_trace_statistics geometry;
+    uint64_t            paths;
+    uint64_t            shadow_rays;
+    uint64_t            scattering_events;
+    uint64_t            roulette_terminations;
+    uint64_t            medium_scattering_events;
+    uint64_t            subsurface_events;
+    double              subsurface_distance;
+} mr_path_statistics;
+
+/* BvhBuildStatistics (include/minirender/render/bvh.hpp:29-34). */
+typedef struct mr_bvh_statistics {
+    uint64_t triangles;
+    uint64_t nodes;
+    uint64_t leaves;
+    uint64_t maximum_depth;
+} mr_bvh_statistics;
+
+/* Ray + RayInterval (include/minirender/scene/scene.hpp:27-30,
+ * include/minirender/render/intersection.hpp:15-20) in FP32: 32 bytes. */
+typedef struct mr_ray {
+    float origin[3];
+    float direction[3];
+    float minimum;
+    float maximum; /* +inf allowed */
+} mr_ray;
+
+/* The part of SurfaceHit (include/minirender/render/bvh.hpp:15-26) that identifies the hit. */
+typedef struct mr_hit {
+    float    distance;
+    uint32_t instance_index;
+    uint32_t triangle_index;
+    uint32_t primitive; /* flat primitive id (instance-major), UINT32_MAX on a miss */
+    float    barycentric[3];
+    uint32_t front_face;
+} mr_hit;
+
+/* RenderProgress (include/minirender/render/render_session.hpp:41-65), path tracing part. */
+typedef struct mr_render_progress {
+    uint32_t           state; /* mr_render_state */
+    uint64_t           job_id;
+    uint64_t           recorded_samples;
+    uint64_t           total_samples;
+    uint64_t           completed_pixels;
+    uint32_t           worker_count;
+    double             elapsed_seconds;
+    mr_path_statistics statistics;
+    char               error[256];
+} mr_render_progress;
+
+/* RenderPreview (include/minirender/render/render_session.hpp:68-77) without the image, which
+ * the caller receives in its own buffer. */
+typedef struct mr_render_preview {
+    uint64_t job_id;
+    uint64_t revision;
+    uint64_t recorded_samples;
+    uint64_t width;
+    uint64_t height;
+    uint32_t available; /* 0 when the preview lock was busy (reference returns no image) */
+} mr_render_preview;
+
+typedef struct mr_scene   mr_scene;
+typedef struct mr_session mr_session;
+
+/* ---- library ---------------------------------------------------------------------------- */
+
+/* ABI version of the loaded library (MR_ABI_VERSION). No reference counterpart. */
+uint32_t mr_abi_version(void);
+
+/* Copies the calling thread's last error message into `buffer` (always NUL-terminated) and
+ * returns its full length. Stands in for the reference's exception `what()` strings. */
+size_t mr_last_error(char* buffer, size_t capacity);
+
+/* ---- scene ------------------------------------------------------------------------------ */
+
+/* Validates the snapshot, uploads it to the current CUDA device and builds everything the
+ * reference's PathTracer constructor builds (src/render/path_tracer.cpp:244-253): the SceneBvh
+ * (src/render/bvh.cpp:141-209; here the GPU binned-SAH builder, or `bvh` when non-null, which
+ * must be the reference layout of the same primitives), the LightSampler
+ * (src/render/light.cpp:340-407) and the MediumField (src/render/medium.cpp:228-231). */
+mr_status mr_scene_create(const mr_scene_desc* desc, const mr_bvh_desc* bvh, mr_scene** scene);
+
+/* Releases every device and host resource of the scene. */
+mr_status mr_scene_destroy(mr_scene* scene);
+
+/* SceneBvh::statistics (include/minirender/render/bvh.hpp:52). */
+mr_status mr_scene_bvh_statistics(const mr_scene* scene, mr_bvh_statistics* statistics);
+
+/* Surface-area-heuristic cost of the scene's BVH with the reference builder's constants
+ * (C_T = C_I = 1, src/render/bvh.cpp:244-245): sum over interior nodes of A(node)/A(root) plus
+ * sum over leaves of count * A(leaf)/A(root). No single reference function computes the
+ * whole-tree figure; it is the cost the reference's split search minimises. */
+mr_status mr_scene_sah_cost(const mr_scene* scene, double* cost);
+
+/* Copies the scene's BVH out in the reference node layout (mr_bvh_node + order). Either
+ * pointer may be null to query the counts only. No reference counterpart (its nodes are
+ * private members, include/minirender/render/bvh.hpp:101-107). */
+mr_status mr_scene_export_bvh(const mr_scene* scene, mr_bvh_node* nodes, uint32_t node_capacity,
+                              uint32_t* order, uint32_t order_capacity, uint32_t* node_count,
+                              uint32_t* primitive_count);
+
+/* Seconds the scene's BVH build took on the device (CUDA events around the build kernels),
+ * 0 for an imported BVH. No reference counterpart (bvh.cpp has no timer; the CLI's
+ * --trace-normals times it, src/app/cli.cpp:60-97). */
+mr_status mr_scene_build_seconds(const mr_scene* scene, double* seconds);
+
+/* ---- queries ---------------------------------------------------------------------------- */
+
+/* SceneBvh::intersect (src/render/bvh.cpp:482-488) for `count` rays: nearest hit in the closed
+ * interval, ties to the lowest primitive id, single-sided culling. */
+mr_status mr_intersect(const mr_scene* scene, const mr_ray* rays, size_t count, mr_hit* hits,
+                       mr_trace_statistics* statistics);
+
+/* SceneBvh::occluded (src/render/bvh.cpp:490-494) for `count` rays; occluded[i] is 0 or 1. */
+mr_status mr_occluded(const mr_scene* scene, const mr_ray* rays, size_t count, uint8_t* occluded,
+                      mr_trace_statistics* statistics);
+
+/* PathTracer::trace (src/render/path_tracer.cpp:286-499) for `count` independent paths. The
+ * sampler of path i is Sampler::for_sample(keys[3i], keys[3i+1], keys[3i+2])
+ * (src/core/sampling.cpp:124-127); rays[i] carries the primary interval. */
+mr_status mr_trace_paths(const mr_scene* scene, const mr_integrator_settings* integrator,
+                         const mr_ray* rays, const uint64_t* keys, size_t count,
+                         float* radiance, mr_path_statistics* statistics);
+
+/* PathTracer::sample_pixel (src/render/path_tracer.cpp:501-519) for `count` (x, y, sample)
+ * triples (`pixels` holds x, y pairs). Writes the radiance and, when `rays` is non-null, the
+ * primary camera ray with its clip interval. */
+mr_status mr_sample_pixels(const mr_scene* scene, const mr_integrator_settings* integrator,
+                           const mr_render_settings* render, const uint32_t* pixels,
+                           const uint64_t* samples, size_t count, float* radiance, mr_ray* rays,
+                           mr_path_statistics* statistics);
+
+/* ---- render ----------------------------------------------------------------------------- */
+
+/* PathTracer::render (src/render/path_tracer.cpp:521-538): writes width*height*3 floats of
+ * linear RGB, row-major, origin top-left (include/minirender/core/image.hpp). Host buffer. */
+mr_status mr_render(const mr_scene* scene, const mr_integrator_settings* integrator,
+                    const mr_render_settings* render, float* rgb, mr_path_statistics* statistics);
+
+/* PathTracer::render with the image left in device memory: `device_rgb` is a device pointer
+ * to width*height*3 floats and `stream` a cudaStream_t (null = the legacy default stream).
+ * The call is asynchronous with respect to the host unless `statistics` is non-null. */
+mr_status mr_render_device(const mr_scene* scene, const mr_integrator_settings* integrator,
+                           const mr_render_settings* render, float* device_rgb, void* stream,
+                           mr_path_statistics* statistics);
+
+/* display_image (src/render/path_tracer.cpp:540-557): exposure + Reinhard on a host image. */
+mr_status mr_display_image(const float* linear, uint64_t width, uint64_t height, double exposure,
+                           float* display);
+
+/* Kernel timing for roofline figures: when enabled, the library records CUDA events around
+ * every launch of the nearest-hit traversal kernel on its launching stream; `mr_kernel_timing`
+ * returns the number of launches, their summed device time in seconds and the summed
+ * bounds/triangle test counters of those launches. No reference counterpart. */
+mr_status mr_set_kernel_timing(int enabled);
+mr_status mr_kernel_timing(uint64_t* launches, double* seconds, mr_trace_statistics* counted);
+
+/* ---- session ---------------------------------------------------------------------------- */
+
+/* RenderSession::RenderSession / ~RenderSession (render_session.hpp:84-87). */
+mr_status mr_session_create(mr_session** session);
+mr_status mr_session_destroy(mr_session* session);
+
+/* RenderSession::start (include/minirender/render/render_session.hpp:91-92). The scene must
+ * outlive the job. MR_LOGIC_ERROR while a job is active. */
+mr_status mr_session_start(mr_session* session, const mr_scene* scene,
+                           const mr_render_settings* render,
+                           const mr_integrator_settings* integrator,
+                           const mr_session_settings* settings);
+
+/* RenderSession::pause / resume (render_session.hpp:93-96): `accepted` receives the bool. */
+mr_status mr_session_pause(mr_session* session, int* accepted);
+mr_status mr_session_resume(mr_session* session, int* accepted);
+
+/* RenderSession::cancel / wait / wait_for (render_session.hpp:97-102). */
+mr_status mr_session_cancel(mr_session* session);
+mr_status mr_session_wait(mr_session* session);
+mr_status mr_session_wait_for(mr_session* session, uint32_t milliseconds, int* terminal);
+
+/* RenderSession::progress (render_session.hpp:104). */
+mr_status mr_session_progress(const mr_session* session, mr_render_progress* progress);
+
+/* RenderSession::preview (render_session.hpp:105-107): fills `rgb` (capacity in floats) with
+ * the preview image of at most `maximum_dimension` on its longer side (0 = full size). */
+mr_status mr_session_preview(const mr_session* session, uint64_t maximum_dimension, float* rgb,
+                             size_t capacity, mr_render_preview* preview);
+
+/* RenderSession::result (render_session.hpp:109): MR_OUT_OF_RANGE unless the job completed. */
+mr_status mr_session_result(const mr_session* session, float* rgb, size_t capacity,
+                            uint64_t* width, uint64_t* height);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MINIRENDER_B200_H */
