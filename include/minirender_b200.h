@@ -189,9 +189,11 @@ typedef struct mr_render_settings {
     uint64_t seed;
 } mr_render_settings;
 
-/* SessionSettings (include/minirender/render/render_session.hpp:30-38). On the GPU `threads` is
- * accepted for validation only; tile_size and batch_samples keep their meaning: one committed
- * unit of work is a tile_size^2 block of pixels advanced by batch_samples samples. */
+/* SessionSettings (include/minirender/render/render_session.hpp:30-38), validated with the
+ * reference's limits. batch_samples keeps its meaning: samples added per pixel between two
+ * commits (progress, preview, pause and cancel points). The GPU advances the whole image per
+ * batch, so `threads` and `tile_size` do not change the schedule; results are bitwise the same
+ * for every setting, as in the reference. */
 typedef struct mr_session_settings {
     uint32_t threads;
     uint32_t tile_size;
@@ -337,6 +339,16 @@ mr_status mr_sample_pixels(const mr_scene* scene, const mr_integrator_settings* 
                            const mr_render_settings* render, const uint32_t* pixels,
                            const uint64_t* samples, size_t count, float* radiance, mr_ray* rays,
                            mr_path_statistics* statistics);
+
+/* Diagnostics for hit-record parity: renders the `count` camera samples like mr_sample_pixels
+ * and reports, per sample, the first shadow ray its path traced (origin, direction, interval
+ * [0, limit]) in `shadow_rays`, has_shadow[i] = 1 when it traced one, and occluded[i] = the
+ * any-hit result. No reference counterpart (the reference traces the same ray inside
+ * PathTracer::shadow_transmittance, src/render/path_tracer.cpp:259-284). */
+mr_status mr_capture_shadow_rays(const mr_scene* scene, const mr_integrator_settings* integrator,
+                                 const mr_render_settings* render, const uint32_t* pixels,
+                                 const uint64_t* samples, size_t count, mr_ray* shadow_rays,
+                                 uint8_t* has_shadow, uint8_t* occluded);
 
 /* ---- render ----------------------------------------------------------------------------- */
 

@@ -181,6 +181,9 @@ SIGNATURES = {
     "mr_sample_pixels": (C.c_int, [VP, P(IntegratorSettings), P(RenderSettings),
                                    P(C.c_uint32), P(C.c_uint64), C.c_size_t, P(C.c_float),
                                    P(Ray), P(PathStatistics)]),
+    "mr_capture_shadow_rays": (C.c_int, [VP, P(IntegratorSettings), P(RenderSettings),
+                                         P(C.c_uint32), P(C.c_uint64), C.c_size_t, P(Ray),
+                                         P(C.c_uint8), P(C.c_uint8)]),
     "mr_render": (C.c_int, [VP, P(IntegratorSettings), P(RenderSettings), P(C.c_float),
                             P(PathStatistics)]),
     "mr_render_device": (C.c_int, [VP, P(IntegratorSettings), P(RenderSettings), VP, VP,

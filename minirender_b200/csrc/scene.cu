@@ -1,0 +1,677 @@
+// scene.cu — validation, upload and device layout of a scene snapshot.
+//
+// Follows the reference's PathTracer construction (src/render/path_tracer.cpp:244-253):
+// snapshot validation (src/scene/scene.cpp:38-66,141-155,241-267; src/scene/medium.cpp:377-420),
+// world-space triangle flattening (src/render/bvh.cpp:141-209), BVH, light table
+// (src/render/light.cpp:340-407) and media. All arithmetic is FP32; the flattening uses
+// explicit unfused multiply/add so host and device produce identical world vertices.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+
+#include "errors.hpp"
+#include "scan.cuh"
+#include "scene.cuh"
+
+namespace mr {
+
+namespace {
+
+// glm::vec3(object_to_world * glm::vec4(p, 1)) in float with GLM's evaluation order
+// (m0*x + m1*y) + (m2*z + m3*w) and no fused operations (src/render/bvh.cpp:178-179).
+MR_HD f3 transform_point(const float* m, float x, float y, float z) {
+#ifdef __CUDA_ARCH__
+    const auto row = [&](int r) {
+        return __fadd_rn(__fadd_rn(__fmul_rn(m[r], x), __fmul_rn(m[4 + r], y)),
+                         __fadd_rn(__fmul_rn(m[8 + r], z), __fmul_rn(m[12 + r], 1.0f)));
+    };
+#else
+    const auto row = [&](int r) {
+        volatile float a = m[r] * x, b = m[4 + r] * y, c = m[8 + r] * z, d = m[12 + r] * 1.0f;
+        volatile float ab = a + b, cd = c + d;
+        return static_cast<float>(ab + cd);
+    };
+#endif
+    return {row(0), row(1), row(2)};
+}
+
+struct DeviceInstance {
+    float    object_to_world[16];
+    float    normal_to_world[9];
+    uint32_t position_offset;
+    uint32_t corner_offset;  // in corners (3 per triangle)
+    uint32_t first_prim;
+    uint32_t triangle_count;
+    uint32_t material;
+    uint32_t flags;  // kTriSingleSided | kTriMirrored | kTriEmissive | kind << 8
+};
+
+__device__ __forceinline__ uint32_t find_instance(const DeviceInstance* instances, uint32_t count,
+                                                  uint32_t prim) {
+    uint32_t lo = 0, hi = count;  // last instance with first_prim <= prim
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (instances[mid].first_prim <= prim) {
+            lo = mid;
+        } else {
+            hi = mid;
+        }
+    }
+    return lo;
+}
+
+// One thread per primitive: world vertices, build bounds/centroid, shading normals, flags.
+__global__ void flatten_kernel(const float* positions, const mr_mesh_corner* corners,
+                               const DeviceInstance* instances, uint32_t instance_count,
+                               uint32_t prim_count, float4* world, float4* shading, float4* lo,
+                               float4* hi, float4* centroid, unsigned* error) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= prim_count) {
+        return;
+    }
+    const uint32_t        ii   = find_instance(instances, instance_count, p);
+    const DeviceInstance& inst = instances[ii];
+    const uint32_t        tri  = p - inst.first_prim;
+    f3                    v[3];
+    f3                    n[3];
+    for (int c = 0; c < 3; ++c) {
+        const mr_mesh_corner& corner = corners[inst.corner_offset + 3 * tri + c];
+        const float*          q      = positions + 3 * (static_cast<size_t>(inst.position_offset) + corner.position);
+        v[c] = transform_point(inst.object_to_world, q[0], q[1], q[2]);
+        const float* m = inst.normal_to_world;
+        const f3 w = {(m[0] * corner.normal[0] + m[3] * corner.normal[1]) + m[6] * corner.normal[2],
+                      (m[1] * corner.normal[0] + m[4] * corner.normal[1]) + m[7] * corner.normal[2],
+                      (m[2] * corner.normal[0] + m[5] * corner.normal[1]) + m[8] * corner.normal[2]};
+        n[c] = normalize(w);
+    }
+    if (!finite3(v[0]) || !finite3(v[1]) || !finite3(v[2])) {
+        atomicOr(error, 1u);
+    }
+    const f3 e1 = v[1] - v[0], e2 = v[2] - v[0];
+    const f3 cr = {difference_of_products(e1.y, e2.z, e2.y, e1.z),
+                   difference_of_products(e1.z, e2.x, e2.z, e1.x),
+                   difference_of_products(e1.x, e2.y, e2.x, e1.y)};
+    if (cr.x == 0 && cr.y == 0 && cr.z == 0) {
+        atomicOr(error, 2u);
+    }
+    world[3 * p + 0] = f4(v[0], __uint_as_float(p));
+    world[3 * p + 1] = f4(v[1], __uint_as_float(inst.flags));
+    world[3 * p + 2] = f4(v[2], 0.0f);
+    shading[3 * p + 0] = f4(n[0], __uint_as_float(ii));
+    shading[3 * p + 1] = f4(n[1], __uint_as_float(tri));
+    shading[3 * p + 2] = f4(n[2], __uint_as_float(inst.material));
+    const f3 mn = {fminf(fminf(v[0].x, v[1].x), v[2].x), fminf(fminf(v[0].y, v[1].y), v[2].y),
+                   fminf(fminf(v[0].z, v[1].z), v[2].z)};
+    const f3 mx = {fmaxf(fmaxf(v[0].x, v[1].x), v[2].x), fmaxf(fmaxf(v[0].y, v[1].y), v[2].y),
+                   fmaxf(fmaxf(v[0].z, v[1].z), v[2].z)};
+    lo[p] = f4(mn, 0.0f);
+    hi[p] = f4(mx, 0.0f);
+    // Centroid as the reference accumulates it: ((v0/3) + v1/3) + v2/3.
+    const f3 third = {((v[0].x / 3.0f) + v[1].x / 3.0f) + v[2].x / 3.0f,
+                      ((v[0].y / 3.0f) + v[1].y / 3.0f) + v[2].y / 3.0f,
+                      ((v[0].z / 3.0f) + v[1].z / 3.0f) + v[2].z / 3.0f};
+    centroid[p] = f4(third, 0.0f);
+}
+
+// Interior-node flags for the rank scan.
+__global__ void interior_flag_kernel(const mr_bvh_node* nodes, uint32_t count, uint32_t* flags) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < count) {
+        flags[i] = nodes[i].count == 0 ? 1u : 0u;
+    }
+}
+
+__device__ __forceinline__ int child_ref(const mr_bvh_node* nodes, const uint32_t* rank,
+                                         uint32_t child) {
+    const mr_bvh_node& c = nodes[child];
+    return c.count == 0 ? static_cast<int>(rank[child]) : ~static_cast<int>(c.first);
+}
+
+// Reference-layout nodes -> traversal nodes (children's boxes stored in the parent).
+__global__ void convert_nodes_kernel(const mr_bvh_node* nodes, const uint32_t* rank,
+                                     uint32_t count, float4* out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count || nodes[i].count != 0) {
+        return;
+    }
+    const mr_bvh_node& l = nodes[nodes[i].first];
+    const mr_bvh_node& r = nodes[nodes[i].right];
+    float4*            o = out + 4 * static_cast<size_t>(rank[i]);
+    o[0] = make_float4(l.minimum[0], l.maximum[0], l.minimum[1], l.maximum[1]);
+    o[1] = make_float4(r.minimum[0], r.maximum[0], r.minimum[1], r.maximum[1]);
+    o[2] = make_float4(l.minimum[2], l.maximum[2], r.minimum[2], r.maximum[2]);
+    o[3] = make_float4(__int_as_float(child_ref(nodes, rank, nodes[i].first)),
+                       __int_as_float(child_ref(nodes, rank, nodes[i].right)), 0.0f, 0.0f);
+}
+
+// Triangle stream in leaf order; marks the last slot of every leaf.
+__global__ void gather_triangles_kernel(const float4* world, const uint32_t* order, uint32_t count,
+                                        float4* tris) {
+    const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= count) {
+        return;
+    }
+    const uint32_t p = order[slot];
+    tris[3 * slot + 0] = world[3 * p + 0];
+    tris[3 * slot + 1] = world[3 * p + 1];
+    tris[3 * slot + 2] = world[3 * p + 2];
+}
+
+__global__ void mark_leaf_end_kernel(const mr_bvh_node* nodes, uint32_t count, float4* tris) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count || nodes[i].count == 0) {
+        return;
+    }
+    float4& t = tris[3 * static_cast<size_t>(nodes[i].first + nodes[i].count - 1) + 1];
+    t.w       = __uint_as_float(__float_as_uint(t.w) | kTriLeafEnd);
+}
+
+bool finite3h(const float* v) { return std::isfinite(v[0]) && std::isfinite(v[1]) && std::isfinite(v[2]); }
+
+float luminance(f3 c) { return (c.x * 0.2126f + c.y * 0.7152f) + c.z * 0.0722f; }
+
+// Camera::validate (src/scene/scene.cpp:141-155).
+void validate_camera(const mr_camera& c) {
+    require(finite3h(c.position) && finite3h(c.target) && finite3h(c.up),
+            "Camera vectors must be finite");
+    const f3 p = {c.position[0], c.position[1], c.position[2]};
+    const f3 t = {c.target[0], c.target[1], c.target[2]};
+    const f3 u = {c.up[0], c.up[1], c.up[2]};
+    require(length(t - p) > 1e-6f, "Camera position and target must differ");
+    require(length(cross(t - p, u)) > 1e-6f, "Camera up must not be parallel to view direction");
+    require(std::isfinite(c.vertical_fov_degrees) && c.vertical_fov_degrees > 0 &&
+                c.vertical_fov_degrees < 179,
+            "Camera FOV must be between 0 and 179 degrees");
+    require(std::isfinite(c.near_plane) && std::isfinite(c.far_plane) && c.near_plane > 0 &&
+                c.far_plane > c.near_plane,
+            "Camera clipping planes must satisfy 0 < near < far");
+    require(std::isfinite(c.aperture_radius) && c.aperture_radius >= 0 &&
+                std::isfinite(c.focus_distance) && c.focus_distance > 0,
+            "Camera lens requires nonnegative aperture and positive focus distance");
+}
+
+// Material::validate (src/scene/scene.cpp:241-267) for the supported kinds.
+void validate_material(const mr_material& m) {
+    require(finite3h(m.base_color) && m.base_color[0] >= 0 && m.base_color[1] >= 0 &&
+                m.base_color[2] >= 0 && m.base_color[0] <= 1 && m.base_color[1] <= 1 &&
+                m.base_color[2] <= 1,
+            "Material base color must be in [0,1]");
+    require(finite3h(m.emission) && m.emission[0] >= 0 && m.emission[1] >= 0 && m.emission[2] >= 0,
+            "Material emission must be nonnegative");
+    require(std::isfinite(m.roughness) && m.roughness >= 0 && m.roughness <= 1,
+            "Roughness must be in [0,1]");
+    require(std::isfinite(m.ior) && m.ior > 0, "IOR must be positive");
+    require(m.kind <= MR_MATERIAL_SUBSURFACE, "Invalid material kind");
+    require(m.kind <= MR_MATERIAL_DIELECTRIC,
+            "Cloth and subsurface materials are not supported by the GPU path tracer");
+}
+
+// MeshData::validate (src/scene/scene.cpp:38-66).
+void validate_mesh(const mr_mesh& m) {
+    require(m.position_count > 0 && m.triangle_count > 0 && m.positions && m.corners,
+            "Mesh must contain positions and triangles");
+    for (uint32_t i = 0; i < m.position_count; ++i) {
+        require(finite3h(m.positions + 3 * i), "Mesh position must be finite");
+    }
+    for (uint32_t t = 0; t < m.triangle_count; ++t) {
+        for (int c = 0; c < 3; ++c) {
+            const mr_mesh_corner& k = m.corners[3 * t + c];
+            require(k.position < m.position_count, "Mesh position index is out of range");
+            const f3 n = {k.normal[0], k.normal[1], k.normal[2]};
+            require(finite3(n) && dot(n, n) > 1e-12f, "Mesh normal must be finite and nonzero");
+            require(std::isfinite(k.uv[0]) && std::isfinite(k.uv[1]), "Mesh UV must be finite");
+        }
+        const float* a = m.positions + 3 * m.corners[3 * t].position;
+        const float* b = m.positions + 3 * m.corners[3 * t + 1].position;
+        const float* c = m.positions + 3 * m.corners[3 * t + 2].position;
+        const f3 e1 = {b[0] - a[0], b[1] - a[1], b[2] - a[2]};
+        const f3 e2 = {c[0] - a[0], c[1] - a[1], c[2] - a[2]};
+        const f3 area = cross(e1, e2);
+        require(dot(area, area) > 1e-20f, "Degenerate mesh triangle");
+    }
+}
+
+// MediumRegion / validate_medium_regions (src/scene/medium.cpp:377-420).
+void validate_media(const mr_medium_region* media, uint32_t count) {
+    require(count <= kMaxMedia, "Scene supports at most 32 medium regions");
+    for (uint32_t i = 0; i < count; ++i) {
+        const auto& r = media[i];
+        bool ok = true;
+        for (int a = 0; a < 3; ++a) {
+            const double e = r.absorption[a] + r.scattering[a];
+            ok = ok && std::isfinite(r.absorption[a]) && std::isfinite(r.scattering[a]) &&
+                 std::isfinite(e) && r.absorption[a] >= 0 && r.scattering[a] >= 0;
+        }
+        require(ok && std::isfinite(r.anisotropy) && std::fabs(r.anisotropy) < 1,
+                "Medium coefficients must be finite/nonnegative and |g| < 1");
+        bool box = true;
+        for (int a = 0; a < 3; ++a) {
+            box = box && std::isfinite(r.minimum[a]) && std::isfinite(r.maximum[a]) &&
+                  std::isfinite(r.maximum[a] - r.minimum[a]) && r.minimum[a] < r.maximum[a];
+        }
+        require(box, "Medium region requires an ID and a finite positive box");
+        if (!r.enabled) {
+            continue;
+        }
+        for (uint32_t j = 0; j < i; ++j) {
+            const auto& o = media[j];
+            if (!o.enabled) {
+                continue;
+            }
+            bool overlap = true;
+            for (int a = 0; a < 3; ++a) {
+                overlap = overlap && std::max(r.minimum[a], o.minimum[a]) < std::min(r.maximum[a], o.maximum[a]);
+            }
+            require(!overlap, "Medium region interiors overlap");
+        }
+    }
+}
+
+float determinant3(const float* m) {
+    const auto e = [m](int c, int r) { return m[4 * c + r]; };
+    return e(0, 0) * (e(1, 1) * e(2, 2) - e(2, 1) * e(1, 2)) -
+           e(1, 0) * (e(0, 1) * e(2, 2) - e(2, 1) * e(0, 2)) +
+           e(2, 0) * (e(0, 1) * e(1, 2) - e(1, 1) * e(0, 2));
+}
+
+void validate_imported(const mr_bvh_desc& b, uint32_t prims) {
+    require(b.primitive_count == prims, "Imported BVH primitive count differs from the scene");
+    require(prims == 0 || (b.node_count > 0 && b.nodes && b.order),
+            "Imported BVH has no nodes");
+    std::vector<uint8_t> seen(prims, 0);
+    for (uint32_t i = 0; i < prims; ++i) {
+        require(b.order[i] < prims && !seen[b.order[i]], "Imported BVH order is not a permutation");
+        seen[b.order[i]] = 1;
+    }
+    std::vector<uint32_t> covered(prims, 0);
+    for (uint32_t i = 0; i < b.node_count; ++i) {
+        const auto& n = b.nodes[i];
+        if (n.count) {
+            require(uint64_t(n.first) + n.count <= prims, "Imported BVH leaf range is out of range");
+            for (uint32_t k = n.first; k < n.first + n.count; ++k) {
+                covered[k]++;
+            }
+        } else {
+            require(n.first < b.node_count && n.right < b.node_count && n.first != i &&
+                        n.right != i,
+                    "Imported BVH child index is out of range");
+        }
+    }
+    for (uint32_t k = 0; k < prims; ++k) {
+        require(covered[k] == 1, "Imported BVH leaves do not cover every slot exactly once");
+    }
+}
+
+}  // namespace
+
+std::unique_ptr<Scene> create_scene(const mr_scene_desc& desc, const mr_bvh_desc* bvh) {
+    int device_count = 0;
+    if (cudaGetDeviceCount(&device_count) != cudaSuccess || device_count == 0) {
+        fail(MR_CUDA_ERROR, "No CUDA device is available");
+    }
+    auto scene = std::make_unique<Scene>();
+    MR_CUDA(cudaGetDevice(&scene->device));
+
+    // ---- validation (make_snapshot) ----
+    validate_camera(desc.camera);
+    require(finite3h(desc.environment) && desc.environment[0] >= 0 && desc.environment[1] >= 0 &&
+                desc.environment[2] >= 0,
+            "Environment must be finite and nonnegative");
+    require(desc.mesh_count == 0 || desc.meshes, "Mesh table is missing");
+    require(desc.material_count == 0 || desc.materials, "Material table is missing");
+    require(desc.instance_count == 0 || desc.instances, "Instance table is missing");
+    for (uint32_t i = 0; i < desc.material_count; ++i) {
+        validate_material(desc.materials[i]);
+    }
+    for (uint32_t i = 0; i < desc.mesh_count; ++i) {
+        validate_mesh(desc.meshes[i]);
+    }
+    validate_media(desc.media, desc.medium_count);
+    for (uint32_t i = 0; i < desc.directional_light_count; ++i) {
+        const auto& l = desc.directional_lights[i];
+        const f3    d = {l.direction[0], l.direction[1], l.direction[2]};
+        require(finite3(d) && length(d) > 1e-6f, "Light direction must be nonzero");
+        require(finite3h(l.color) && l.color[0] >= 0 && l.color[1] >= 0 && l.color[2] >= 0 &&
+                    std::isfinite(l.intensity) && l.intensity >= 0,
+                "Light color/intensity must be nonnegative");
+    }
+    uint64_t total = 0;
+    std::vector<DeviceInstance> instances(desc.instance_count);
+    std::vector<uint32_t> mesh_position_offset(desc.mesh_count), mesh_corner_offset(desc.mesh_count);
+    uint64_t positions_total = 0, corners_total = 0;
+    for (uint32_t m = 0; m < desc.mesh_count; ++m) {
+        mesh_position_offset[m] = static_cast<uint32_t>(positions_total);
+        mesh_corner_offset[m]   = static_cast<uint32_t>(corners_total);
+        positions_total += desc.meshes[m].position_count;
+        corners_total += 3ull * desc.meshes[m].triangle_count;
+        if (positions_total > 0xffffffffull || corners_total > 0xffffffffull) {
+            fail(MR_LENGTH_ERROR, "Scene mesh data exceeds the 32-bit index range");
+        }
+    }
+    for (uint32_t i = 0; i < desc.instance_count; ++i) {
+        const mr_instance& in = desc.instances[i];
+        require(in.mesh < desc.mesh_count, "Object references missing mesh");
+        require(in.material < desc.material_count, "Object references missing material");
+        bool finite = true;
+        for (int k = 0; k < 16; ++k) finite = finite && std::isfinite(in.object_to_world[k]);
+        for (int k = 0; k < 9; ++k) finite = finite && std::isfinite(in.normal_to_world[k]);
+        require(finite, "Transform must be finite");
+        const uint32_t tris = desc.meshes[in.mesh].triangle_count;
+        if (tris > 0x7fffffffull - total) {
+            fail(MR_LENGTH_ERROR, "Scene triangle count exceeds BVH index range");
+        }
+        DeviceInstance& d = instances[i];
+        std::memcpy(d.object_to_world, in.object_to_world, sizeof(d.object_to_world));
+        std::memcpy(d.normal_to_world, in.normal_to_world, sizeof(d.normal_to_world));
+        d.position_offset = mesh_position_offset[in.mesh];
+        d.corner_offset   = mesh_corner_offset[in.mesh];
+        d.first_prim      = static_cast<uint32_t>(total);
+        d.triangle_count  = tris;
+        d.material        = in.material;
+        const mr_material& mat = desc.materials[in.material];
+        d.flags = (mat.double_sided ? 0u : kTriSingleSided) |
+                  (determinant3(in.object_to_world) < 0 ? kTriMirrored : 0u) |
+                  ((mat.emission[0] > 0 || mat.emission[1] > 0 || mat.emission[2] > 0) ? kTriEmissive : 0u) |
+                  (mat.kind << 8);
+        total += tris;
+    }
+    const uint32_t prims = static_cast<uint32_t>(total);
+    scene->d.primitive_count = prims;
+    if (bvh) {
+        validate_imported(*bvh, prims);
+    }
+
+    cudaStream_t stream = nullptr;
+    size_t       bytes  = 0;
+
+    // ---- upload meshes and instances ----
+    DeviceBuffer<float>          positions;
+    DeviceBuffer<mr_mesh_corner> corners;
+    DeviceBuffer<uint8_t>        instance_buffer;
+    positions.allocate(3 * positions_total);
+    corners.allocate(corners_total);
+    for (uint32_t m = 0; m < desc.mesh_count; ++m) {
+        const mr_mesh& mesh = desc.meshes[m];
+        MR_CUDA(cudaMemcpyAsync(positions.ptr + 3ull * mesh_position_offset[m], mesh.positions,
+                                3ull * mesh.position_count * sizeof(float), cudaMemcpyHostToDevice, stream));
+        MR_CUDA(cudaMemcpyAsync(corners.ptr + mesh_corner_offset[m], mesh.corners,
+                                3ull * mesh.triangle_count * sizeof(mr_mesh_corner),
+                                cudaMemcpyHostToDevice, stream));
+    }
+    instance_buffer.allocate(std::max<size_t>(1, instances.size() * sizeof(DeviceInstance)));
+    if (!instances.empty()) {
+        MR_CUDA(cudaMemcpyAsync(instance_buffer.ptr, instances.data(),
+                                instances.size() * sizeof(DeviceInstance), cudaMemcpyHostToDevice, stream));
+    }
+
+    // ---- flatten ----
+    DeviceBuffer<float4>   world, lo, hi, centroid;
+    DeviceBuffer<uint32_t> error;
+    world.allocate(3ull * prims);
+    scene->shading.allocate(3ull * prims);
+    lo.allocate(prims);
+    hi.allocate(prims);
+    centroid.allocate(prims);
+    error.allocate(1);
+    MR_CUDA(cudaMemsetAsync(error.ptr, 0, sizeof(uint32_t), stream));
+    if (prims) {
+        flatten_kernel<<<(prims + 255) / 256, 256, 0, stream>>>(
+            positions.ptr, corners.ptr, reinterpret_cast<const DeviceInstance*>(instance_buffer.ptr),
+            desc.instance_count, prims, world.ptr, scene->shading.ptr, lo.ptr, hi.ptr, centroid.ptr,
+            error.ptr);
+        MR_CUDA(cudaGetLastError());
+    }
+    uint32_t flatten_error = 0;
+    MR_CUDA(cudaMemcpyAsync(&flatten_error, error.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+    MR_CUDA(cudaStreamSynchronize(stream));
+    require(!(flatten_error & 1u), "Transformed triangle position is not finite");
+    require(!(flatten_error & 2u), "Transform collapses a triangle at float precision");
+    positions.release();
+    corners.release();
+
+    // ---- BVH (reference layout on the device) ----
+    DeviceBuffer<mr_bvh_node> ref_nodes;
+    DeviceBuffer<uint32_t>    ref_order;
+    uint32_t                  node_count = 0;
+    if (prims) {
+        if (bvh) {
+            node_count = bvh->node_count;
+            ref_nodes.allocate(node_count);
+            ref_order.allocate(prims);
+            MR_CUDA(cudaMemcpyAsync(ref_nodes.ptr, bvh->nodes, node_count * sizeof(mr_bvh_node),
+                                    cudaMemcpyHostToDevice, stream));
+            MR_CUDA(cudaMemcpyAsync(ref_order.ptr, bvh->order, prims * sizeof(uint32_t),
+                                    cudaMemcpyHostToDevice, stream));
+            // Statistics of the imported tree (host walk).
+            std::vector<std::pair<uint32_t, uint32_t>> stack{{0u, 0u}};
+            uint64_t leaves = 0, depth = 0;
+            while (!stack.empty()) {
+                const auto [i, d] = stack.back();
+                stack.pop_back();
+                depth = std::max<uint64_t>(depth, d);
+                const auto& n = bvh->nodes[i];
+                if (n.count) {
+                    ++leaves;
+                } else {
+                    require(d < 64, "Imported BVH is deeper than 64 levels");
+                    stack.push_back({n.first, d + 1});
+                    stack.push_back({n.right, d + 1});
+                }
+            }
+            scene->statistics.leaves        = leaves;
+            scene->statistics.maximum_depth = depth;
+        } else {
+            BuildResult built = build_bvh_device(lo.ptr, hi.ptr, centroid.ptr, prims, stream);
+            ref_nodes             = std::move(built.nodes);
+            ref_order             = std::move(built.order);
+            node_count            = built.node_count;
+            scene->statistics.leaves        = built.leaves;
+            scene->statistics.maximum_depth = built.maximum_depth;
+            scene->build_seconds  = built.seconds;
+        }
+    }
+    scene->statistics.triangles = prims;
+    scene->statistics.nodes     = node_count;
+    lo.release();
+    hi.release();
+    centroid.release();
+
+    // ---- traversal layout ----
+    uint32_t interior = 0;
+    if (prims) {
+        DeviceBuffer<uint32_t> flags, rank, scratch, total_interior;
+        flags.allocate(node_count);
+        rank.allocate(node_count);
+        scratch.allocate(scan_scratch_size(node_count));
+        total_interior.allocate(1);
+        interior_flag_kernel<<<(node_count + 255) / 256, 256, 0, stream>>>(ref_nodes.ptr, node_count, flags.ptr);
+        exclusive_scan(flags.ptr, rank.ptr, node_count, scratch.ptr, total_interior.ptr, stream);
+        MR_CUDA(cudaMemcpyAsync(&interior, total_interior.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+        MR_CUDA(cudaStreamSynchronize(stream));
+        scene->nodes.allocate(std::max<uint32_t>(1, interior) * 4ull);
+        if (interior) {
+            convert_nodes_kernel<<<(node_count + 255) / 256, 256, 0, stream>>>(ref_nodes.ptr, rank.ptr,
+                                                                                 node_count, scene->nodes.ptr);
+        }
+        scene->tris.allocate(3ull * prims);
+        gather_triangles_kernel<<<(prims + 255) / 256, 256, 0, stream>>>(world.ptr, ref_order.ptr, prims,
+                                                                         scene->tris.ptr);
+        mark_leaf_end_kernel<<<(node_count + 255) / 256, 256, 0, stream>>>(ref_nodes.ptr, node_count,
+                                                                           scene->tris.ptr);
+        MR_CUDA(cudaGetLastError());
+        mr_bvh_node root{};
+        MR_CUDA(cudaMemcpyAsync(&root, ref_nodes.ptr, sizeof(root), cudaMemcpyDeviceToHost, stream));
+        MR_CUDA(cudaStreamSynchronize(stream));
+        scene->d.has_nodes  = 1;
+        scene->d.root       = root.count == 0 ? 0 : ~static_cast<int>(root.first);
+        scene->d.root_count = root.count;
+        for (int a = 0; a < 3; ++a) {
+            scene->d.root_lo[a] = root.minimum[a];
+            scene->d.root_hi[a] = root.maximum[a];
+        }
+    }
+    scene->d.node_count = interior;
+    scene->ref_nodes    = std::move(ref_nodes);
+    scene->ref_order    = std::move(ref_order);
+
+    // ---- materials ----
+    std::vector<DeviceMaterial> materials(std::max<uint32_t>(1, desc.material_count));
+    for (uint32_t i = 0; i < desc.material_count; ++i) {
+        const mr_material& m = desc.materials[i];
+        materials[i] = {{m.base_color[0], m.base_color[1], m.base_color[2]},
+                        {m.emission[0], m.emission[1], m.emission[2]},
+                        m.roughness * m.roughness, m.ior, m.kind, m.double_sided};
+    }
+    scene->materials.allocate(materials.size());
+    MR_CUDA(cudaMemcpyAsync(scene->materials.ptr, materials.data(), materials.size() * sizeof(DeviceMaterial),
+                            cudaMemcpyHostToDevice, stream));
+
+    // ---- lights (LightSampler constructor, src/render/light.cpp:340-407) ----
+    std::vector<DeviceLight> lights;
+    std::vector<float>       weights;
+    std::vector<uint32_t>    emitter_of_prim(std::max<uint32_t>(1, prims), kNone);
+    for (uint32_t i = 0; i < desc.instance_count; ++i) {
+        const mr_instance& in  = desc.instances[i];
+        const mr_material& mat = desc.materials[in.material];
+        const f3 radiance = {mat.emission[0], mat.emission[1], mat.emission[2]};
+        if (luminance(radiance) == 0) {
+            continue;
+        }
+        const mr_mesh& mesh        = desc.meshes[in.mesh];
+        const float    orientation = determinant3(in.object_to_world) < 0 ? -1.0f : 1.0f;
+        for (uint32_t t = 0; t < mesh.triangle_count; ++t) {
+            f3 v[3];
+            for (int c = 0; c < 3; ++c) {
+                const float* p = mesh.positions + 3 * mesh.corners[3 * t + c].position;
+                v[c]           = transform_point(in.object_to_world, p[0], p[1], p[2]);
+            }
+            const f3    cr   = cross(v[1] - v[0], v[2] - v[0]);
+            const float area = length(cr) * 0.5f;
+            if (area == 0) {
+                continue;
+            }
+            DeviceLight l{};
+            l.v0 = v[0];
+            l.v1 = v[1];
+            l.v2 = v[2];
+            l.normal       = cr * orientation / (2.0f * area);
+            l.radiance     = radiance;
+            l.area         = area;
+            l.kind         = kLightArea;
+            l.double_sided = mat.double_sided;
+            emitter_of_prim[instances[i].first_prim + t] = static_cast<uint32_t>(lights.size());
+            lights.push_back(l);
+            weights.push_back((mat.double_sided ? 2.0f : 1.0f) * kPi * area * luminance(radiance));
+        }
+    }
+    float projected_area = kPi;
+    if (prims) {
+        const f3 extent = {scene->d.root_hi[0] - scene->d.root_lo[0], scene->d.root_hi[1] - scene->d.root_lo[1],
+                           scene->d.root_hi[2] - scene->d.root_lo[2]};
+        projected_area = kPi * std::max(dot(extent, extent) * 0.25f, 1e-12f);
+    }
+    for (uint32_t i = 0; i < desc.directional_light_count; ++i) {
+        const auto& dl       = desc.directional_lights[i];
+        const f3    radiance = f3{dl.color[0], dl.color[1], dl.color[2]} * dl.intensity;
+        if (luminance(radiance) > 0) {
+            DeviceLight l{};
+            l.normal   = -normalize(f3{dl.direction[0], dl.direction[1], dl.direction[2]});
+            l.radiance = radiance;
+            l.kind     = kLightDirectional;
+            lights.push_back(l);
+            weights.push_back(projected_area * luminance(radiance));
+        }
+    }
+    const f3 environment = {desc.environment[0], desc.environment[1], desc.environment[2]};
+    scene->d.environment        = environment;
+    scene->d.environment_choice = -1;
+    const float integral        = 4.0f * kPi * luminance(environment);
+    if (integral > 0) {
+        DeviceLight l{};
+        l.radiance = environment;
+        l.kind     = kLightEnvironment;
+        scene->d.environment_choice = static_cast<int>(lights.size());
+        lights.push_back(l);
+        weights.push_back(projected_area * integral);
+    }
+    // DiscreteDistribution (src/core/sampling.cpp:190-208) in FP32.
+    std::vector<float> cdf(weights.size() + 1, 0.0f);
+    float maximum = 0;
+    for (float w : weights) {
+        require(std::isfinite(w) && w >= 0, "Distribution weights must be finite and nonnegative");
+        maximum = std::max(maximum, w);
+    }
+    for (size_t i = 0; i < weights.size(); ++i) {
+        cdf[i + 1] = cdf[i] + (maximum > 0 ? weights[i] / maximum : 1.0f);
+    }
+    if (!weights.empty()) {
+        const float integral_cdf = cdf.back();
+        for (auto& v : cdf) {
+            v /= integral_cdf;
+        }
+    }
+    scene->d.light_count = static_cast<uint32_t>(lights.size());
+    scene->lights.allocate(std::max<size_t>(1, lights.size()));
+    scene->light_cdf.allocate(cdf.size());
+    scene->prim_emitter.allocate(emitter_of_prim.size());
+    if (!lights.empty()) {
+        MR_CUDA(cudaMemcpyAsync(scene->lights.ptr, lights.data(), lights.size() * sizeof(DeviceLight),
+                                cudaMemcpyHostToDevice, stream));
+    }
+    MR_CUDA(cudaMemcpyAsync(scene->light_cdf.ptr, cdf.data(), cdf.size() * sizeof(float),
+                            cudaMemcpyHostToDevice, stream));
+    MR_CUDA(cudaMemcpyAsync(scene->prim_emitter.ptr, emitter_of_prim.data(),
+                            emitter_of_prim.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+
+    // ---- media ----
+    std::vector<DeviceMedium> media(std::max<uint32_t>(1, desc.medium_count));
+    int scatter = 0;
+    for (uint32_t i = 0; i < desc.medium_count; ++i) {
+        const auto& r = desc.media[i];
+        DeviceMedium& m = media[i];
+        m.minimum    = {float(r.minimum[0]), float(r.minimum[1]), float(r.minimum[2])};
+        m.maximum    = {float(r.maximum[0]), float(r.maximum[1]), float(r.maximum[2])};
+        m.absorption = {float(r.absorption[0]), float(r.absorption[1]), float(r.absorption[2])};
+        m.scattering = {float(r.scattering[0]), float(r.scattering[1]), float(r.scattering[2])};
+        m.extinction = m.absorption + m.scattering;
+        m.anisotropy = float(r.anisotropy);
+        m.scatters   = (m.scattering.x != 0 || m.scattering.y != 0 || m.scattering.z != 0) ? 1 : 0;
+        m.enabled    = r.enabled ? 1 : 0;
+        scatter |= m.scatters && m.enabled;
+    }
+    scene->media.allocate(media.size());
+    MR_CUDA(cudaMemcpyAsync(scene->media.ptr, media.data(), media.size() * sizeof(DeviceMedium),
+                            cudaMemcpyHostToDevice, stream));
+    scene->d.medium_count  = static_cast<int>(desc.medium_count);
+    scene->d.media_scatter = scatter;
+
+    // ---- camera basis (src/scene/scene.cpp:176-180) ----
+    const mr_camera& c = desc.camera;
+    CameraBasis&     b = scene->d.camera;
+    b.position        = {c.position[0], c.position[1], c.position[2]};
+    b.forward         = normalize(f3{c.target[0], c.target[1], c.target[2]} - b.position);
+    b.right           = normalize(cross(b.forward, f3{c.up[0], c.up[1], c.up[2]}));
+    b.up              = cross(b.right, b.forward);
+    b.half_height     = std::tan(c.vertical_fov_degrees * (kPi / 180.0f) * 0.5f);
+    b.near_plane      = c.near_plane;
+    b.far_plane       = c.far_plane;
+    b.aperture_radius = c.aperture_radius;
+    b.focus_distance  = c.focus_distance;
+
+    MR_CUDA(cudaStreamSynchronize(stream));
+    scene->d.nodes        = scene->nodes.ptr;
+    scene->d.tris         = scene->tris.ptr;
+    scene->d.shading      = scene->shading.ptr;
+    scene->d.materials    = scene->materials.ptr;
+    scene->d.lights       = scene->lights.ptr;
+    scene->d.light_cdf    = scene->light_cdf.ptr;
+    scene->d.prim_emitter = scene->prim_emitter.ptr;
+    scene->d.media        = scene->media.ptr;
+    bytes = scene->nodes.bytes() + scene->tris.bytes() + scene->shading.bytes() +
+            scene->ref_nodes.bytes() + scene->ref_order.bytes() + scene->prim_emitter.bytes();
+    scene->device_bytes = bytes;
+    return scene;
+}
+
+}  // namespace mr

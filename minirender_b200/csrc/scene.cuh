@@ -1,0 +1,86 @@
+// scene.cuh — host-side scene object behind the opaque mr_scene handle.
+#pragma once
+
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "device_scene.cuh"
+#include "errors.hpp"
+
+namespace mr {
+
+// Owning device allocation (cudaMalloc/cudaFree), movable only.
+template <typename T> struct DeviceBuffer {
+    T*     ptr   = nullptr;
+    size_t count = 0;
+    DeviceBuffer() = default;
+    DeviceBuffer(const DeviceBuffer&) = delete;
+    DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+    DeviceBuffer(DeviceBuffer&& o) noexcept : ptr(o.ptr), count(o.count) { o.ptr = nullptr; o.count = 0; }
+    DeviceBuffer& operator=(DeviceBuffer&& o) noexcept {
+        release();
+        ptr = o.ptr;
+        count = o.count;
+        o.ptr = nullptr;
+        o.count = 0;
+        return *this;
+    }
+    ~DeviceBuffer() { release(); }
+    void release() {
+        if (ptr) {
+            cudaFree(ptr);
+            ptr   = nullptr;
+            count = 0;
+        }
+    }
+    void allocate(size_t n) {  // throws Error (MR_OUT_OF_MEMORY / MR_CUDA_ERROR)
+        release();
+        if (n == 0) {
+            return;
+        }
+        MR_CUDA(cudaMalloc(reinterpret_cast<void**>(&ptr), n * sizeof(T)));
+        count = n;
+    }
+    size_t bytes() const { return count * sizeof(T); }
+};
+
+struct Scene {
+    int         device = 0;
+    DeviceScene d{};
+
+    DeviceBuffer<float4>         nodes;
+    DeviceBuffer<float4>         tris;
+    DeviceBuffer<float4>         shading;
+    DeviceBuffer<DeviceMaterial> materials;
+    DeviceBuffer<DeviceLight>    lights;
+    DeviceBuffer<float>          light_cdf;
+    DeviceBuffer<uint32_t>       prim_emitter;
+    DeviceBuffer<DeviceMedium>   media;
+
+    // Reference-layout BVH (mr_bvh_node + order) kept on the device for export and SAH.
+    DeviceBuffer<mr_bvh_node> ref_nodes;
+    DeviceBuffer<uint32_t>    ref_order;
+    mr_bvh_statistics        statistics{};
+    double                   build_seconds = 0;
+    double                   sah_cost      = 0;
+    size_t                   device_bytes  = 0;
+};
+
+// Scene construction (scene.cu).
+std::unique_ptr<Scene> create_scene(const mr_scene_desc& desc, const mr_bvh_desc* bvh);
+
+// GPU binned-SAH builder (builder.cu): from per-primitive FP32 bounds and centroids on the
+// device to a reference-layout tree (DFS-independent node numbering, root at index 0).
+struct BuildResult {
+    DeviceBuffer<mr_bvh_node> nodes;
+    DeviceBuffer<uint32_t>    order;
+    uint32_t                  node_count    = 0;
+    uint64_t                  leaves        = 0;
+    uint64_t                  maximum_depth = 0;
+    double                    seconds       = 0;
+};
+BuildResult build_bvh_device(const float4* lo, const float4* hi, const float4* centroid,
+                             uint32_t count, cudaStream_t stream);
+
+}  // namespace mr

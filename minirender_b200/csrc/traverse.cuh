@@ -1,0 +1,249 @@
+// traverse.cuh — FP32 ray queries over the BVH: slab test, watertight triangle test, nearest and
+// any-hit traversal.
+//
+// Semantics follow the reference exactly (src/render/intersection.cpp, src/render/bvh.cpp:316-410):
+// closed intervals, ties to the lower primitive id, single-sided culling by geometric winding,
+// any-hit exit on the first accepted triangle, pruning of popped subtrees whose entry distance
+// exceeds the current nearest hit. Differences are numeric only:
+//  - slab distances are widened by 2^-20 relative instead of one double ulp, so the box test
+//    stays conservative in FP32 (FP32 rounding of (b - o) * inv is at most a few ulps);
+//  - the triangle test is the same permute/shear/difference-of-products algorithm in FP32 with
+//    the error bound of the reference evaluated with FP32's unit roundoff.
+#pragma once
+
+#include "device_scene.cuh"
+
+namespace mr {
+
+constexpr int      kStackSize  = 64;  // trees are at most 48 levels deep (bvh.cpp:126)
+
+struct RayQuery {
+    f3    o, d;
+    float inv_lo[3];  // 1/d scaled down by 2^-20: near slab distances round toward the origin
+    float inv_hi[3];  // 1/d scaled up by 2^-20: far slab distances round away
+    bool  neg[3];     // direction sign per axis (the near slab is the max bound)
+    int   kx, ky, kz;
+    float sx, sy, sz;
+
+    __device__ __forceinline__ void init(f3 origin, f3 direction) {
+        o = origin;
+        d = direction;
+        const float lo = 0.99999904632568359375f;  // 1 - 2^-20
+        const float hi = 1.00000095367431640625f;  // 1 + 2^-20
+        for (int a = 0; a < 3; ++a) {
+            const float c = comp(d, a);
+            const float inv = 1.0f / c;  // +-inf for +-0: the slab then imposes no bound
+            inv_lo[a] = inv * lo;
+            inv_hi[a] = inv * hi;
+            neg[a]    = signbit(c);
+        }
+        // Permutation and shear (src/render/intersection.cpp:130-145).
+        const f3 ad = fabs3(d);
+        kz          = ad.x > ad.y ? 0 : 1;
+        if (ad.z > comp(ad, kz)) {
+            kz = 2;
+        }
+        kx = kz == 2 ? 0 : kz + 1;
+        ky = kx == 2 ? 0 : kx + 1;
+        if (comp(d, kz) < 0) {
+            const int t = kx;
+            kx          = ky;
+            ky          = t;
+        }
+        const float dz = comp(d, kz);
+        sx             = comp(d, kx) / dz;
+        sy             = comp(d, ky) / dz;
+        sz             = 1.0f / dz;
+    }
+};
+
+// Entry distance of one child box, or +inf when the slab intervals do not overlap within
+// [tmin, tmax]. `xy` = (lo.x, hi.x, lo.y, hi.y); (zlo, zhi) the z extent.
+__device__ __forceinline__ float slab_enter(const RayQuery& q, float4 xy, float zlo, float zhi,
+                                            float tmin, float tmax) {
+    const float nx = ((q.neg[0] ? xy.y : xy.x) - q.o.x) * q.inv_lo[0];
+    const float fx = ((q.neg[0] ? xy.x : xy.y) - q.o.x) * q.inv_hi[0];
+    const float ny = ((q.neg[1] ? xy.w : xy.z) - q.o.y) * q.inv_lo[1];
+    const float fy = ((q.neg[1] ? xy.z : xy.w) - q.o.y) * q.inv_hi[1];
+    const float nz = ((q.neg[2] ? zhi : zlo) - q.o.z) * q.inv_lo[2];
+    const float fz = ((q.neg[2] ? zlo : zhi) - q.o.z) * q.inv_hi[2];
+    // fmaxf/fminf ignore the NaN of 0 * inf (origin on the slab plane of a zero component).
+    const float enter = fmaxf(fmaxf(tmin, nx), fmaxf(ny, nz));
+    const float leave = fminf(fminf(tmax, fx), fminf(fy, fz));
+    return enter <= leave ? enter : __int_as_float(0x7f800000);
+}
+
+__device__ __forceinline__ float permuted(f3 v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
+
+// Watertight triangle test (src/render/intersection.cpp:179-223) in FP32. On acceptance returns
+// the distance and the three unnormalised edge functions plus their sum (the determinant).
+__device__ __forceinline__ bool triangle_test(const RayQuery& q, f3 v0, f3 v1, f3 v2, float tmin,
+                                              float tmax, float& t, float& ea, float& eb,
+                                              float& ec, float& det) {
+    const f3 t0 = v0 - q.o, t1 = v1 - q.o, t2 = v2 - q.o;
+    const float z0 = permuted(t0, q.kz), z1 = permuted(t1, q.kz), z2 = permuted(t2, q.kz);
+    const float p0x = fmaf(-q.sx, z0, permuted(t0, q.kx));
+    const float p0y = fmaf(-q.sy, z0, permuted(t0, q.ky));
+    const float p1x = fmaf(-q.sx, z1, permuted(t1, q.kx));
+    const float p1y = fmaf(-q.sy, z1, permuted(t1, q.ky));
+    const float p2x = fmaf(-q.sx, z2, permuted(t2, q.kx));
+    const float p2y = fmaf(-q.sy, z2, permuted(t2, q.ky));
+    const float a = difference_of_products(p1x, p2y, p1y, p2x);
+    const float b = difference_of_products(p2x, p0y, p2y, p0x);
+    const float c = difference_of_products(p0x, p1y, p0y, p1x);
+    if ((a < 0 || b < 0 || c < 0) && (a > 0 || b > 0 || c > 0)) {
+        return false;
+    }
+    const float determinant = a + b + c;
+    if (determinant == 0) {
+        return false;
+    }
+    const float pz0 = z0 * q.sz, pz1 = z1 * q.sz, pz2 = z2 * q.sz;
+    const float distance = __fdiv_rn(a * pz0 + b * pz1 + c * pz2, determinant);
+    if (!(distance >= tmin && distance <= tmax)) {
+        return false;
+    }
+    // Error bound of PBRT 4 section 6.5.3 with FP32's unit roundoff u = 2^-24.
+    constexpr float g2 = 2.0f * 5.9604644775390625e-08f / (1.0f - 2.0f * 5.9604644775390625e-08f);
+    constexpr float g3 = 3.0f * 5.9604644775390625e-08f / (1.0f - 3.0f * 5.9604644775390625e-08f);
+    constexpr float g5 = 5.0f * 5.9604644775390625e-08f / (1.0f - 5.0f * 5.9604644775390625e-08f);
+    const float x = fmaxf(fmaxf(fabsf(p0x), fabsf(p1x)), fabsf(p2x));
+    const float y = fmaxf(fmaxf(fabsf(p0y), fabsf(p1y)), fabsf(p2y));
+    const float z = fmaxf(fmaxf(fabsf(pz0), fabsf(pz1)), fabsf(pz2));
+    const float error_x    = g5 * (x + z);
+    const float error_y    = g5 * (y + z);
+    const float error_edge = 2.0f * (g2 * x * y + error_y * x + error_x * y);
+    const float edge       = fmaxf(fmaxf(fabsf(a), fabsf(b)), fabsf(c));
+    const float error_distance =
+        3.0f * (g3 * edge * z + error_edge * z + g3 * z * edge) / fabsf(determinant);
+    if (distance <= error_distance) {
+        return false;
+    }
+    t   = distance;
+    ea  = a;
+    eb  = b;
+    ec  = c;
+    det = determinant;
+    return true;
+}
+
+struct TraceResult {
+    float    t;
+    uint32_t slot;  // triangle slot in leaf order, kNone for a miss
+    uint32_t prim;
+    float    a, b, c, det;
+};
+
+struct TraceCounters {
+    uint32_t bounds;
+    uint32_t triangles;
+};
+
+// Nearest hit (ANY_HIT = false) or occlusion (ANY_HIT = true) in [tmin, tmax].
+template <bool ANY_HIT>
+__device__ __forceinline__ TraceResult trace(const DeviceScene& s, const RayQuery& q, float tmin,
+                                             float tmax, TraceCounters& counters,
+                                             unsigned& error) {
+    TraceResult result;
+    result.t    = tmax;
+    result.slot = kNone;
+    result.prim = kNone;
+    if (!s.has_nodes) {
+        return result;
+    }
+    // The root's own box (src/render/bvh.cpp:331-334).
+    counters.bounds++;
+    const float root_enter =
+        slab_enter(q, make_float4(s.root_lo[0], s.root_hi[0], s.root_lo[1], s.root_hi[1]),
+                   s.root_lo[2], s.root_hi[2], tmin, tmax);
+    if (!(root_enter <= tmax)) {
+        return result;
+    }
+    int2  stack[kStackSize];
+    int   sp        = 0;
+    int   node      = s.root;
+    float node_tmin = root_enter;
+    while (true) {
+        if (node >= 0) {
+            const float4* n  = s.nodes + 4 * static_cast<size_t>(node);
+            const float4  lxy = __ldg(n + 0);
+            const float4  rxy = __ldg(n + 1);
+            const float4  z   = __ldg(n + 2);
+            const int4    lk  = __ldg(reinterpret_cast<const int4*>(n + 3));
+            counters.bounds += 2;
+            const float tl = slab_enter(q, lxy, z.x, z.y, tmin, result.t);
+            const float tr = slab_enter(q, rxy, z.z, z.w, tmin, result.t);
+            const bool  hl = tl <= result.t;
+            const bool  hr = tr <= result.t;
+            if (hl && hr) {
+                const bool left_nearer = tl <= tr;
+                if (sp == kStackSize) {
+                    error |= kErrorStack;
+                    return result;
+                }
+                stack[sp++] = left_nearer ? make_int2(lk.y, __float_as_int(tr))
+                                          : make_int2(lk.x, __float_as_int(tl));
+                node      = left_nearer ? lk.x : lk.y;
+                node_tmin = left_nearer ? tl : tr;
+                continue;
+            }
+            if (hl || hr) {
+                node      = hl ? lk.x : lk.y;
+                node_tmin = hl ? tl : tr;
+                continue;
+            }
+        } else {
+            // Leaf: triangles from slot ~node until the leaf-end flag.
+            for (uint32_t slot = static_cast<uint32_t>(~node);; ++slot) {
+                const float4* tp = s.tris + 3 * static_cast<size_t>(slot);
+                const float4  a4 = __ldg(tp + 0);
+                const float4  b4 = __ldg(tp + 1);
+                const float4  c4 = __ldg(tp + 2);
+                const unsigned flags = __float_as_uint(b4.w);
+                counters.triangles++;
+                float t, ea, eb, ec, det;
+                if (triangle_test(q, xyz(a4), xyz(b4), xyz(c4), tmin, result.t, t, ea, eb, ec,
+                                  det)) {
+                    bool visible = true;
+                    if (flags & kTriSingleSided) {
+                        // Outward normal from the winding (src/render/bvh.cpp:369-381).
+                        const f3 outward = cross(xyz(b4) - xyz(a4), xyz(c4) - xyz(a4));
+                        const float side = dot(q.d, outward);
+                        visible = (flags & kTriMirrored) ? side > 0 : side < 0;
+                    }
+                    const uint32_t prim = __float_as_uint(a4.w);
+                    if (visible && (t < result.t || (t == result.t && prim < result.prim) ||
+                                    result.slot == kNone)) {
+                        result.t    = t;
+                        result.slot = slot;
+                        result.prim = prim;
+                        result.a    = ea;
+                        result.b    = eb;
+                        result.c    = ec;
+                        result.det  = det;
+                        if (ANY_HIT) {
+                            return result;
+                        }
+                    }
+                }
+                if (flags & kTriLeafEnd) {
+                    break;
+                }
+            }
+        }
+        // Pop the next subtree that can still contain a nearer hit.
+        while (true) {
+            if (sp == 0) {
+                return result;
+            }
+            const int2 e = stack[--sp];
+            node_tmin    = __int_as_float(e.y);
+            node         = e.x;
+            if (node_tmin <= result.t) {
+                break;
+            }
+        }
+    }
+}
+
+}  // namespace mr

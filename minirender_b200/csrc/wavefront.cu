@@ -1,0 +1,941 @@
+// wavefront.cu — wavefront path tracing on the GPU.
+//
+// One wave = up to `capacity` camera paths. Each bounce runs three persistent kernels:
+//   extend  nearest-hit traversal of the bounce's ray queue; classifies every path into a
+//           material bin (miss, diffuse, conductor, mirror, dielectric, medium) with
+//           warp-aggregated appends (match_any + popc + one atomic per key per warp);
+//   shade   emission with MIS, next-event estimation, BSDF sampling and Russian roulette,
+//           processed bin by bin so warps execute one material's code; appends the shadow
+//           queue and the next bounce's ray queue;
+//   shadow  any-hit traversal of the shadow queue, adding the unoccluded contributions.
+// The per-path logic is PathTracer::trace (src/render/path_tracer.cpp:286-499) in FP32 with the
+// reference's RNG stream layout; every path writes only its own state, so images do not depend
+// on scheduling. Radiance is kept per path and added to the pixels in sample order after the
+// wave (compensated FP32 sums), so a frame is deterministic.
+#include <algorithm>
+#include <cstring>
+#include <memory>
+#include <string>
+
+#include "errors.hpp"
+#include "shading.cuh"
+#include "wavefront.cuh"
+
+namespace mr {
+
+namespace {
+
+struct KernelArgs {
+    DeviceScene      scene;
+    PathState        st;
+    Queues           q;
+    IntegratorParams p;
+    uint32_t         capacity;
+    uint32_t         bounce;
+    uint8_t*         occluded_out;  // diagnostics: per-path occlusion of this bounce's shadow ray
+};
+
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31; }
+
+// Appends `value` to queue[key] (key == kNone: nothing) with one atomic per distinct key per
+// warp. Must be called by all 32 lanes.
+__device__ __forceinline__ void warp_append(uint32_t key, uint32_t value, uint32_t* counts,
+                                            uint32_t* queues, size_t stride) {
+    const unsigned peers = __match_any_sync(0xffffffffu, key);
+    if (key == kNone) {
+        return;
+    }
+    const int lane   = lane_id();
+    const int leader = __ffs(peers) - 1;
+    uint32_t  base   = 0;
+    if (lane == leader) {
+        base = atomicAdd(counts + key, static_cast<uint32_t>(__popc(peers)));
+    }
+    base               = __shfl_sync(peers, base, leader);
+    const uint32_t pos = base + __popc(peers & ((1u << lane) - 1u));
+    queues[key * stride + pos] = value;
+}
+
+__device__ __forceinline__ void warp_add_stat(unsigned long long* stat, uint32_t value) {
+    const uint32_t total = __reduce_add_sync(0xffffffffu, value);
+    if (lane_id() == 0 && total) {
+        atomicAdd(stat, static_cast<unsigned long long>(total));
+    }
+}
+
+__device__ __forceinline__ Pcg32 load_rng(const PathState& st, uint32_t path) {
+    const ulonglong2 r = st.rng[path];
+    return {r.x, r.y};
+}
+
+__device__ __forceinline__ void store_rng(const PathState& st, uint32_t path, const Pcg32& r) {
+    st.rng[path] = make_ulonglong2(r.state, r.increment);
+}
+
+__device__ __forceinline__ void init_path(const KernelArgs& a, uint32_t slot, Pcg32 rng, f3 o, f3 d,
+                                          float tmin, float tmax) {
+    a.st.rng[slot]      = make_ulonglong2(rng.state, rng.increment);
+    a.st.ray_o[slot]    = f4(o, tmin);
+    a.st.ray_d[slot]    = f4(d, tmax);
+    a.st.beta[slot]     = make_float4(1, 1, 1, 1);
+    a.st.radiance[slot] = make_float4(0, 0, 0, 0);
+    a.st.prev[slot]     = make_float4(0, 0, 0, 0);
+    a.st.flags[slot]    = 1u;  // previous_delta = true
+    a.q.ext[0][slot]    = slot;
+}
+
+// Camera paths of a pixel rectangle x sample range (PathTracer::sample_pixel,
+// src/render/path_tracer.cpp:501-519).
+__global__ void init_camera_kernel(KernelArgs a, WaveInit w) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t n = w.count;
+    if (i >= n) {
+        return;
+    }
+    uint32_t x, y;
+    uint64_t sample;
+    if (w.kind == kInitCamera) {
+        const uint32_t area = w.w * w.h;
+        const uint32_t s    = i / area;
+        const uint32_t r    = i - s * area;
+        const uint32_t ry   = r / w.w;
+        x                   = w.x0 + (r - ry * w.w);
+        y                   = w.y0 + ry;
+        sample              = w.s0 + s;
+    } else {
+        x      = w.pixels[2 * i];
+        y      = w.pixels[2 * i + 1];
+        sample = w.samples[i];
+    }
+    Pcg32       rng   = Pcg32::for_sample(w.seed, static_cast<uint64_t>(y) * w.width + x, sample);
+    const float fx    = rng.next_1d();
+    const float fy    = rng.next_1d();
+    const float lx    = rng.next_1d();
+    const float ly    = rng.next_1d();
+    const float u     = (static_cast<float>(x) + fx) / static_cast<float>(w.width);
+    const float v     = (static_cast<float>(y) + fy) / static_cast<float>(w.height);
+    const float aspect = static_cast<float>(w.width) / static_cast<float>(w.height);
+    const CameraRay r = camera_ray(a.scene.camera, u, v, aspect, lx, ly);
+    init_path(a, i, rng, r.origin, r.direction, r.minimum, r.maximum);
+    if (w.camera_rays_out) {
+        w.camera_rays_out[2 * i]     = f4(r.origin, r.minimum);
+        w.camera_rays_out[2 * i + 1] = f4(r.direction, r.maximum);
+    }
+    if (i == 0) {
+        a.q.counters[0].ext = n;
+    }
+    if (lane_id() == 0) {
+        atomicAdd(a.q.stats + kStatPaths,
+                  static_cast<unsigned long long>(min(32u, n - (i & ~31u))));
+    }
+}
+
+// Paths with caller rays and stream keys (PathTracer::trace).
+__global__ void init_rays_kernel(KernelArgs a, WaveInit w) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= w.count) {
+        return;
+    }
+    const Pcg32  rng = Pcg32::for_sample(w.keys[3 * i], w.keys[3 * i + 1], w.keys[3 * i + 2]);
+    const float4 o   = w.rays[2 * i];
+    const float4 d   = w.rays[2 * i + 1];
+    init_path(a, i, rng, xyz(o), xyz(d), o.w, d.w);
+    if (i == 0) {
+        a.q.counters[0].ext = w.count;
+    }
+    if (lane_id() == 0) {
+        atomicAdd(a.q.stats + kStatPaths,
+                  static_cast<unsigned long long>(min(32u, w.count - (i & ~31u))));
+    }
+}
+
+// ---- extend ----
+
+template <bool MEDIA>
+__global__ void __launch_bounds__(128) extend_kernel(KernelArgs a) {
+    BounceCounters* ctr   = a.q.counters + a.bounce;
+    const uint32_t  count = ctr->ext;
+    const uint32_t* in    = a.q.ext[a.bounce & 1];
+    TraceCounters   tc{0, 0};
+    unsigned        error = 0;
+    const int       lane  = lane_id();
+    while (true) {
+        uint32_t base = 0;
+        if (lane == 0) {
+            base = atomicAdd(&ctr->work_extend, 32u);
+        }
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= count) {
+            break;
+        }
+        const uint32_t i   = base + lane;
+        uint32_t       key = kNone;
+        uint32_t       path = 0;
+        if (i < count) {
+            path            = in[i];
+            const float4 o4 = a.st.ray_o[path];
+            const float4 d4 = a.st.ray_d[path];
+            RayQuery     q;
+            q.init(xyz(o4), xyz(d4));
+            const TraceResult r = trace<false>(a.scene, q, o4.w, d4.w, tc, error);
+            uint32_t          kind = 0;
+            if (r.slot != kNone) {
+                a.st.hit[path] = make_float4(r.t, __fdiv_rn(r.a, r.det), __fdiv_rn(r.b, r.det),
+                                             __fdiv_rn(r.c, r.det));
+                kind = (__float_as_uint(__ldg(a.scene.tris + 3 * static_cast<size_t>(r.slot) + 1).w) >> 8) & 0xffu;
+            }
+            a.st.hit_slot[path] = r.slot;
+            key = r.slot == kNone ? kBinMiss : kBinDiffuse + kind;
+            if (MEDIA && a.scene.medium_count > 0) {
+                // MediumField::sample over [minimum, hit ? distance : maximum]
+                // (src/render/path_tracer.cpp:303-310).
+                Pcg32  rng   = load_rng(a.st, path);
+                float4 beta4 = a.st.beta[path];
+                bool   scattered;
+                float  scatter_t = 0, g = 0;
+                const f3 w = field_sample(a.scene, xyz(o4), xyz(d4), o4.w,
+                                          r.slot != kNone ? r.t : d4.w, rng, scattered, scatter_t, g,
+                                          error);
+                f3 beta = xyz(beta4) * w;
+                store_rng(a.st, path, rng);
+                a.st.beta[path] = f4(beta, beta4.w);
+                if (!finite3(beta) || beta.x < 0 || beta.y < 0 || beta.z < 0) {
+                    error |= kErrorRadiance;
+                    key = kNone;
+                } else if (max3(beta) == 0) {
+                    key = kNone;
+                } else if (scattered) {
+                    a.st.hit[path] = make_float4(scatter_t, g, 0, 0);
+                    key            = kBinMedium;
+                }
+            }
+        }
+        warp_append(key, path, ctr->bins, a.q.bins, a.capacity);
+    }
+    warp_add_stat(a.q.stats + kStatExtendBounds, tc.bounds);
+    warp_add_stat(a.q.stats + kStatExtendTriangles, tc.triangles);
+    if (error) {
+        atomicOr(a.q.error, error);
+    }
+}
+
+// ---- shade ----
+
+struct ShadeResult {
+    bool continue_path;
+    bool shadow;
+};
+
+__device__ __forceinline__ float emission_weight(const IntegratorParams& p, uint32_t depth,
+                                                 bool previous_delta, float previous_pdf,
+                                                 float light_pdf) {
+    if (depth == 0 || previous_delta || p.mode == MR_SAMPLING_BSDF) {
+        return 1.0f;
+    }
+    return p.mode == MR_SAMPLING_MIS ? power_heuristic(previous_pdf, light_pdf) : 0.0f;
+}
+
+// Russian roulette (src/render/path_tracer.cpp:485-495). Returns false when the path ends.
+__device__ __forceinline__ bool roulette(const IntegratorParams& p, uint32_t depth, Pcg32& rng,
+                                         f3& beta, float eta_scale, uint32_t& rr_count) {
+    const float u = rng.next_1d();
+    if (p.russian_roulette && depth + 1 >= p.roulette_depth) {
+        const float survival = fminf(fmaxf(max3(beta * eta_scale), 0.05f), 0.95f);
+        if (u >= survival) {
+            ++rr_count;
+            return false;
+        }
+        beta = beta * (1.0f / survival);
+    }
+    return true;
+}
+
+struct ShadeStats {
+    uint32_t shadow_rays = 0, scattering = 0, roulette = 0, medium = 0;
+};
+
+__device__ ShadeResult shade_surface(const KernelArgs& a, uint32_t path, int bin, ShadeStats& stats,
+                                     unsigned& error) {
+    const DeviceScene&      s     = a.scene;
+    const IntegratorParams& p     = a.p;
+    const uint32_t          depth = a.bounce;
+    const float4            d4    = a.st.ray_d[path];
+    const f3                dir   = xyz(d4);
+    const float4            beta4 = a.st.beta[path];
+    f3                      beta  = xyz(beta4);
+    float                   eta_scale = beta4.w;
+    const float4            prev4 = a.st.prev[path];
+    const bool              previous_delta = a.st.flags[path] & 1u;
+    float4                  L4    = a.st.radiance[path];
+    f3                      L     = xyz(L4);
+    ShadeResult             out{false, false};
+
+    if (bin == kBinMiss) {
+        L += beta * s.environment *
+             emission_weight(p, depth, previous_delta, prev4.w, environment_pdf(s));
+        a.st.radiance[path] = f4(L, 0);
+        return out;
+    }
+    Pcg32 rng = load_rng(a.st, path);
+    if (bin == kBinMedium) {
+        // Medium vertex (src/render/path_tracer.cpp:311-356).
+        const float4 h      = a.st.hit[path];
+        const float4 o4     = a.st.ray_o[path];
+        const f3     vertex = xyz(o4) + h.x * dir;
+        const float  g      = h.y;
+        if (depth == p.maximum_depth) {
+            return out;
+        }
+        const f3    wo      = -dir;
+        const float light_u = rng.next_1d();
+        const float lsx     = rng.next_1d();
+        const float lsy     = rng.next_1d();
+        const float phx     = rng.next_1d();
+        const float phy     = rng.next_1d();
+        LightSample ls;
+        if (sample_light(s, vertex, light_u, lsx, lsy, ls) &&
+            (p.mode != MR_SAMPLING_BSDF || ls.discrete)) {
+            const float phase = henyey_greenstein(wo, ls.direction, g);
+            ++stats.shadow_rays;
+            f3    sd;
+            float limit;
+            if (shadow_segment(vertex, ls, sd, limit)) {
+                float weight = 1.0f;
+                if (p.mode == MR_SAMPLING_MIS && !ls.discrete) {
+                    weight = power_heuristic(ls.probability, phase);
+                }
+                a.st.shadow_o[path] = f4(vertex, limit);
+                a.st.shadow_d[path] = f4(sd, 0);
+                a.st.shadow_c[path] = f4(beta * ls.radiance * (phase * weight / ls.probability), 0);
+                out.shadow          = true;
+            }
+        }
+        float     pdf;
+        const f3  next = sample_henyey_greenstein(wo, g, phx, phy, pdf);
+        ++stats.scattering;
+        ++stats.medium;
+        if (!roulette(p, depth, rng, beta, eta_scale, stats.roulette)) {
+            store_rng(a.st, path, rng);
+            return out;
+        }
+        a.st.prev[path]  = f4(vertex, pdf);
+        a.st.flags[path] = 0u;
+        a.st.ray_o[path] = f4(vertex, 0.0f);
+        a.st.ray_d[path] = f4(next, INFINITY);
+        a.st.beta[path]  = f4(beta, eta_scale);
+        store_rng(a.st, path, rng);
+        out.continue_path = true;
+        return out;
+    }
+
+    // Surface vertex (src/render/path_tracer.cpp:357-496).
+    const float4     h   = a.st.hit[path];
+    const uint32_t   slot = a.st.hit_slot[path];
+    const SurfaceHit sh  = surface_hit(s, dir, slot, h.y, h.z, h.w);
+    const DeviceMaterial m = s.materials[sh.material];
+    if (m.emission.x > 0 || m.emission.y > 0 || m.emission.z > 0) {
+        L += beta * m.emission *
+             emission_weight(p, depth, previous_delta, prev4.w,
+                             area_pdf(s, xyz(prev4), sh.prim, sh.position));
+        a.st.radiance[path] = f4(L, 0);
+    }
+    if (depth == p.maximum_depth) {
+        return out;
+    }
+    const f3 wo_world = -dir;
+    f3       normal   = m.kind == MR_MATERIAL_DIELECTRIC ? sh.geometric_normal : sh.shading_normal;
+    if (dot(normal, wo_world) < 0) {
+        normal = -normal;
+    }
+    Frame frame;
+    frame.init(normal);
+    const f3 wo = frame.to_local(wo_world);
+    Bsdf     bsdf;
+    bsdf.init(m, sh.front_face);
+    const float light_u   = rng.next_1d();
+    const float sux       = rng.next_1d();
+    const float suy       = rng.next_1d();
+    const float component = rng.next_1d();
+    const float dux       = rng.next_1d();
+    const float duy       = rng.next_1d();
+    if (!bsdf.is_delta()) {
+        LightSample ls;
+        if (sample_light(s, sh.position, light_u, sux, suy, ls) &&
+            (p.mode != MR_SAMPLING_BSDF || ls.discrete)) {
+            const f3   wi = frame.to_local(ls.direction);
+            const bool reflection_side =
+                dot(wo_world, sh.geometric_normal) * dot(ls.direction, sh.geometric_normal) > 0;
+            if (wi.z > 0 && reflection_side) {
+                ++stats.shadow_rays;
+                const f3 origin =
+                    offset_origin(sh.position, sh.geometric_normal, sh.position_error, ls.direction);
+                LightSample lsn = ls;
+                lsn.direction   = normalize(ls.direction);
+                f3    sd;
+                float limit;
+                if (shadow_segment(origin, lsn, sd, limit)) {
+                    float weight = 1.0f;
+                    if (p.mode == MR_SAMPLING_MIS && !ls.discrete) {
+                        weight = power_heuristic(ls.probability, bsdf.pdf(wo, wi));
+                    }
+                    a.st.shadow_o[path] = f4(origin, limit);
+                    a.st.shadow_d[path] = f4(sd, 0);
+                    a.st.shadow_c[path] = f4(beta * bsdf.evaluate(wo, wi) * wi.z * ls.radiance *
+                                                 (weight / ls.probability),
+                                             0);
+                    out.shadow = true;
+                }
+            }
+        }
+    }
+    Bsdf::Sample sample;
+    if (!bsdf.sample(wo, component, dux, duy, sample) || max3(sample.weight) == 0) {
+        store_rng(a.st, path, rng);
+        return out;
+    }
+    const f3    wi_world = normalize(frame.to_world(sample.direction));
+    const float sides    = dot(wo_world, sh.geometric_normal) * dot(wi_world, sh.geometric_normal);
+    if ((sample.transmission && sides >= 0) || (!sample.transmission && sides <= 0)) {
+        store_rng(a.st, path, rng);
+        return out;
+    }
+    beta = beta * sample.weight;
+    if (!finite3(beta) || beta.x < 0 || beta.y < 0 || beta.z < 0) {
+        error |= kErrorRadiance;
+        return out;
+    }
+    eta_scale *= sample.eta * sample.eta;
+    ++stats.scattering;
+    const f3 origin = offset_origin(sh.position, sh.geometric_normal, sh.position_error, wi_world);
+    const f3 next   = normalize(wi_world);
+    if (!roulette(p, depth, rng, beta, eta_scale, stats.roulette)) {
+        store_rng(a.st, path, rng);
+        return out;
+    }
+    a.st.prev[path]  = f4(sh.position, sample.probability);
+    a.st.flags[path] = sample.discrete ? 1u : 0u;
+    a.st.ray_o[path] = f4(origin, 0.0f);
+    a.st.ray_d[path] = f4(next, INFINITY);
+    a.st.beta[path]  = f4(beta, eta_scale);
+    store_rng(a.st, path, rng);
+    out.continue_path = true;
+    return out;
+}
+
+__global__ void __launch_bounds__(128) shade_kernel(KernelArgs a) {
+    BounceCounters* ctr = a.q.counters + a.bounce;
+    uint32_t        prefix[kBinCount + 1];
+    prefix[0] = 0;
+    for (int k = 0; k < kBinCount; ++k) {
+        prefix[k + 1] = prefix[k] + ctr->bins[k];
+    }
+    const uint32_t total  = prefix[kBinCount];
+    uint32_t*      next   = a.q.ext[(a.bounce + 1) & 1];
+    BounceCounters* nctr  = a.q.counters + a.bounce + 1;
+    ShadeStats     stats;
+    unsigned       error  = 0;
+    const uint32_t warps  = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t warp   = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    for (uint32_t base = warp * 32; base < total; base += warps * 32) {
+        const uint32_t i      = base + lane_id();
+        uint32_t       path   = 0;
+        uint32_t       ext_key = kNone, shadow_key = kNone;
+        if (i < total) {
+            int bin = 0;
+            while (i >= prefix[bin + 1]) {
+                ++bin;
+            }
+            path                 = a.q.bins[bin * static_cast<size_t>(a.capacity) + (i - prefix[bin])];
+            const ShadeResult r  = shade_surface(a, path, bin, stats, error);
+            ext_key              = r.continue_path ? 0u : kNone;
+            shadow_key           = r.shadow ? 0u : kNone;
+        }
+        warp_append(shadow_key, path, &ctr->shadow, a.q.shadow, 0);
+        warp_append(ext_key, path, &nctr->ext, next, 0);
+    }
+    warp_add_stat(a.q.stats + kStatShadowRays, stats.shadow_rays);
+    warp_add_stat(a.q.stats + kStatScattering, stats.scattering);
+    warp_add_stat(a.q.stats + kStatRoulette, stats.roulette);
+    warp_add_stat(a.q.stats + kStatMedium, stats.medium);
+    if (error) {
+        atomicOr(a.q.error, error);
+    }
+}
+
+// ---- shadow ----
+
+template <bool MEDIA>
+__global__ void __launch_bounds__(128) shadow_kernel(KernelArgs a) {
+    BounceCounters* ctr   = a.q.counters + a.bounce;
+    const uint32_t  count = ctr->shadow;
+    TraceCounters   tc{0, 0};
+    unsigned        error = 0;
+    const int       lane  = lane_id();
+    while (true) {
+        uint32_t base = 0;
+        if (lane == 0) {
+            base = atomicAdd(&ctr->work_shadow, 32u);
+        }
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= count) {
+            break;
+        }
+        const uint32_t i = base + lane;
+        if (i < count) {
+            const uint32_t path = a.q.shadow[i];
+            const float4   o4   = a.st.shadow_o[path];
+            const float4   d4   = a.st.shadow_d[path];
+            RayQuery       q;
+            q.init(xyz(o4), xyz(d4));
+            const TraceResult r = trace<true>(a.scene, q, 0.0f, o4.w, tc, error);
+            if (a.occluded_out) {
+                a.occluded_out[path] = r.slot != kNone ? 1 : 0;
+            }
+            if (r.slot == kNone) {
+                f3 c = xyz(a.st.shadow_c[path]);
+                if (MEDIA && a.scene.medium_count > 0) {
+                    c = c * field_transmittance(a.scene, xyz(o4), xyz(d4), 0.0f, o4.w);
+                }
+                float4 L = a.st.radiance[path];
+                a.st.radiance[path] = make_float4(L.x + c.x, L.y + c.y, L.z + c.z, 0);
+            }
+        }
+    }
+    warp_add_stat(a.q.stats + kStatShadowBounds, tc.bounds);
+    warp_add_stat(a.q.stats + kStatShadowTriangles, tc.triangles);
+    if (error) {
+        atomicOr(a.q.error, error);
+    }
+}
+
+// ---- pixel accumulation ----
+
+__device__ __forceinline__ void neumaier(float& sum, float& comp, float v) {
+    const float t = sum + v;
+    comp += fabsf(sum) >= fabsf(v) ? (sum - t) + v : (v - t) + sum;
+    sum = t;
+}
+
+// Adds the wave's per-path radiance to the pixels in sample order; checks every path result
+// like check_radiance (src/render/path_tracer.cpp:155-159).
+__global__ void resolve_kernel(const float4* radiance, uint32_t x0, uint32_t y0, uint32_t w,
+                               uint32_t h, uint32_t ns, uint32_t width, float4* accumulator,
+                               unsigned* error) {
+    const uint32_t r    = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t area = w * h;
+    if (r >= area) {
+        return;
+    }
+    const uint32_t ry    = r / w;
+    const size_t   pixel = static_cast<size_t>(y0 + ry) * width + x0 + (r - ry * w);
+    float4         sum   = accumulator[2 * pixel];
+    float4         comp  = accumulator[2 * pixel + 1];
+    bool           bad   = false;
+    for (uint32_t s = 0; s < ns; ++s) {
+        const float4 v = radiance[static_cast<size_t>(s) * area + r];
+        bad |= !(isfinite(v.x) && isfinite(v.y) && isfinite(v.z)) || v.x < 0 || v.y < 0 || v.z < 0;
+        neumaier(sum.x, comp.x, v.x);
+        neumaier(sum.y, comp.y, v.y);
+        neumaier(sum.z, comp.z, v.z);
+    }
+    if (bad) {
+        atomicOr(error, kErrorRadiance);
+    }
+    accumulator[2 * pixel]     = sum;
+    accumulator[2 * pixel + 1] = comp;
+}
+
+// Pixel mean and the overflow check of PathTracer::render (src/render/path_tracer.cpp:527-534).
+__global__ void finalize_kernel(const float4* accumulator, size_t pixels, uint32_t spp, float* rgb,
+                                unsigned* error) {
+    const size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= pixels) {
+        return;
+    }
+    const float4 s = accumulator[2 * i];
+    const float4 c = accumulator[2 * i + 1];
+    const float  n = static_cast<float>(spp);
+    const float  r = (s.x + c.x) / n, g = (s.y + c.y) / n, b = (s.z + c.z) / n;
+    if (!(isfinite(r) && isfinite(g) && isfinite(b))) {
+        atomicOr(error, kErrorOverflow);
+    }
+    rgb[3 * i]     = r;
+    rgb[3 * i + 1] = g;
+    rgb[3 * i + 2] = b;
+}
+
+// Diagnostics: copies the first-bounce shadow rays of the queued paths.
+__global__ void capture_shadow_kernel(KernelArgs a, float4* rays, uint8_t* has_shadow) {
+    const uint32_t count = a.q.counters[0].shadow;
+    const uint32_t i     = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < count) {
+        const uint32_t path = a.q.shadow[i];
+        rays[2 * path]      = a.st.shadow_o[path];
+        rays[2 * path + 1]  = a.st.shadow_d[path];
+        has_shadow[path]    = 1;
+    }
+}
+
+__global__ void copy_radiance_kernel(const float4* radiance, uint32_t count, float* out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < count) {
+        const float4 v = radiance[i];
+        out[3 * i]     = v.x;
+        out[3 * i + 1] = v.y;
+        out[3 * i + 2] = v.z;
+    }
+}
+
+// ---- launch helpers ----
+
+struct LaunchShape {
+    int extend_blocks[2]  = {0, 0};
+    int shade_blocks      = 0;
+    int shadow_blocks[2]  = {0, 0};
+};
+
+LaunchShape& launch_shape() {
+    static thread_local int         device = -1;
+    static thread_local LaunchShape shape;
+    int current = 0;
+    cudaGetDevice(&current);
+    if (device != current) {
+        int sms = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, current);
+        int per = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, extend_kernel<false>, 128, 0);
+        shape.extend_blocks[0] = sms * std::max(1, per);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, extend_kernel<true>, 128, 0);
+        shape.extend_blocks[1] = sms * std::max(1, per);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, shade_kernel, 128, 0);
+        shape.shade_blocks = sms * std::max(1, per);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, shadow_kernel<false>, 128, 0);
+        shape.shadow_blocks[0] = sms * std::max(1, per);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, shadow_kernel<true>, 128, 0);
+        shape.shadow_blocks[1] = sms * std::max(1, per);
+        device = current;
+    }
+    return shape;
+}
+
+size_t align_up(size_t v) { return (v + 255) & ~size_t(255); }
+
+}  // namespace
+
+KernelTiming& kernel_timing() {
+    static KernelTiming timing;
+    return timing;
+}
+
+Workspace::~Workspace() {
+    if (memory) {
+        cudaFree(memory);
+    }
+}
+
+namespace {
+
+std::shared_ptr<Workspace> allocate_workspace(size_t capacity, uint32_t max_bounces, size_t pixels) {
+    auto   ws     = std::make_shared<Workspace>();
+    size_t offset = 0;
+    const auto field = [&](size_t bytes) {
+        const size_t at = offset;
+        offset += align_up(bytes);
+        return at;
+    };
+    const size_t o_rng = field(capacity * sizeof(ulonglong2));
+    const size_t o_beta = field(capacity * sizeof(float4));
+    const size_t o_rad = field(capacity * sizeof(float4));
+    const size_t o_prev = field(capacity * sizeof(float4));
+    const size_t o_flags = field(capacity * sizeof(uint32_t));
+    const size_t o_ro = field(capacity * sizeof(float4));
+    const size_t o_rd = field(capacity * sizeof(float4));
+    const size_t o_hit = field(capacity * sizeof(float4));
+    const size_t o_slot = field(capacity * sizeof(uint32_t));
+    const size_t o_so = field(capacity * sizeof(float4));
+    const size_t o_sd = field(capacity * sizeof(float4));
+    const size_t o_sc = field(capacity * sizeof(float4));
+    const size_t o_e0 = field(capacity * sizeof(uint32_t));
+    const size_t o_e1 = field(capacity * sizeof(uint32_t));
+    const size_t o_bins = field(capacity * kBinCount * sizeof(uint32_t));
+    const size_t o_shadow = field(capacity * sizeof(uint32_t));
+    const size_t o_ctr = field((max_bounces + 2) * sizeof(BounceCounters));
+    const size_t o_stats = field(kStatCount * sizeof(unsigned long long));
+    const size_t o_err = field(sizeof(unsigned));
+    const size_t o_acc = field(2 * pixels * sizeof(float4));
+    void*        mem   = nullptr;
+    MR_CUDA(cudaMalloc(&mem, offset));
+    char* base              = static_cast<char*>(mem);
+    ws->memory              = mem;
+    ws->bytes               = offset;
+    ws->capacity            = capacity;
+    ws->max_bounces         = max_bounces;
+    ws->pixels              = pixels;
+    ws->state.rng           = reinterpret_cast<ulonglong2*>(base + o_rng);
+    ws->state.beta          = reinterpret_cast<float4*>(base + o_beta);
+    ws->state.radiance      = reinterpret_cast<float4*>(base + o_rad);
+    ws->state.prev          = reinterpret_cast<float4*>(base + o_prev);
+    ws->state.flags         = reinterpret_cast<uint32_t*>(base + o_flags);
+    ws->state.ray_o         = reinterpret_cast<float4*>(base + o_ro);
+    ws->state.ray_d         = reinterpret_cast<float4*>(base + o_rd);
+    ws->state.hit           = reinterpret_cast<float4*>(base + o_hit);
+    ws->state.hit_slot      = reinterpret_cast<uint32_t*>(base + o_slot);
+    ws->state.shadow_o      = reinterpret_cast<float4*>(base + o_so);
+    ws->state.shadow_d      = reinterpret_cast<float4*>(base + o_sd);
+    ws->state.shadow_c      = reinterpret_cast<float4*>(base + o_sc);
+    ws->queues.ext[0]       = reinterpret_cast<uint32_t*>(base + o_e0);
+    ws->queues.ext[1]       = reinterpret_cast<uint32_t*>(base + o_e1);
+    ws->queues.bins         = reinterpret_cast<uint32_t*>(base + o_bins);
+    ws->queues.shadow       = reinterpret_cast<uint32_t*>(base + o_shadow);
+    ws->queues.counters     = reinterpret_cast<BounceCounters*>(base + o_ctr);
+    ws->queues.stats        = reinterpret_cast<unsigned long long*>(base + o_stats);
+    ws->queues.error        = reinterpret_cast<unsigned*>(base + o_err);
+    ws->accumulator         = reinterpret_cast<float4*>(base + o_acc);
+    return ws;
+}
+
+std::mutex                              pool_mutex;
+std::vector<std::shared_ptr<Workspace>> pool;
+
+}  // namespace
+
+std::shared_ptr<Workspace> acquire_workspace(size_t capacity, uint32_t max_bounces, size_t pixels) {
+    int device = 0;
+    MR_CUDA(cudaGetDevice(&device));
+    {
+        std::lock_guard<std::mutex> lock(pool_mutex);
+        for (size_t i = 0; i < pool.size(); ++i) {
+            auto& w = pool[i];
+            int   d = -1;
+            cudaPointerAttributes attr{};
+            if (cudaPointerGetAttributes(&attr, w->memory) == cudaSuccess) {
+                d = attr.device;
+            }
+            if (d == device && w->capacity >= capacity && w->max_bounces >= max_bounces &&
+                w->pixels >= pixels) {
+                auto out = w;
+                pool.erase(pool.begin() + static_cast<long>(i));
+                return out;
+            }
+        }
+    }
+    cudaGetLastError();
+    return allocate_workspace(capacity, max_bounces, pixels);
+}
+
+void release_workspace(std::shared_ptr<Workspace> ws) {
+    if (!ws) {
+        return;
+    }
+    std::lock_guard<std::mutex> lock(pool_mutex);
+    pool.push_back(std::move(ws));
+    if (pool.size() > 4) {
+        pool.erase(pool.begin());
+    }
+}
+
+void reset_statistics(Workspace& ws, cudaStream_t stream) {
+    MR_CUDA(cudaMemsetAsync(ws.queues.stats, 0, kStatCount * sizeof(unsigned long long), stream));
+    MR_CUDA(cudaMemsetAsync(ws.queues.error, 0, sizeof(unsigned), stream));
+}
+
+void read_statistics(Workspace& ws, cudaStream_t stream, mr_path_statistics* out, unsigned* error) {
+    unsigned long long stats[kStatCount];
+    unsigned           e = 0;
+    MR_CUDA(cudaMemcpyAsync(stats, ws.queues.stats, sizeof(stats), cudaMemcpyDeviceToHost, stream));
+    MR_CUDA(cudaMemcpyAsync(&e, ws.queues.error, sizeof(e), cudaMemcpyDeviceToHost, stream));
+    MR_CUDA(cudaStreamSynchronize(stream));
+    if (out) {
+        std::memset(out, 0, sizeof(*out));
+        out->paths                    = stats[kStatPaths];
+        out->shadow_rays              = stats[kStatShadowRays];
+        out->scattering_events        = stats[kStatScattering];
+        out->roulette_terminations    = stats[kStatRoulette];
+        out->medium_scattering_events = stats[kStatMedium];
+        out->geometry.bounds_tests    = stats[kStatExtendBounds] + stats[kStatShadowBounds];
+        out->geometry.triangle_tests  = stats[kStatExtendTriangles] + stats[kStatShadowTriangles];
+    }
+    if (error) {
+        *error = e;
+    }
+}
+
+mr_status error_status(unsigned error, std::string& message) {
+    if (error & kErrorOverflow) {
+        message = "Rendered radiance exceeds the float image range";
+        return MR_OVERFLOW;
+    }
+    if (error & kErrorRadiance) {
+        message = "Path contribution is nonfinite or negative";
+        return MR_RUNTIME_ERROR;
+    }
+    if (error & kErrorMedium) {
+        message = "Medium sample has zero mixture probability";
+        return MR_RUNTIME_ERROR;
+    }
+    if (error & kErrorStack) {
+        message = "BVH traversal stack exhausted";
+        return MR_RUNTIME_ERROR;
+    }
+    return MR_OK;
+}
+
+void Engine::run_wave(const Scene& scene, const IntegratorParams& params, const WaveInit& init,
+                      Workspace& ws, cudaStream_t stream) {
+    if (init.count == 0) {
+        return;
+    }
+    if (init.count > ws.capacity || params.maximum_depth + 1 > ws.max_bounces) {
+        fail(MR_LENGTH_ERROR, "Wave exceeds the workspace capacity");
+    }
+    KernelArgs a;
+    a.scene    = scene.d;
+    a.st       = ws.state;
+    a.q        = ws.queues;
+    a.p        = params;
+    a.capacity = static_cast<uint32_t>(ws.capacity);
+    a.bounce   = 0;
+    a.occluded_out = nullptr;
+    MR_CUDA(cudaMemsetAsync(ws.queues.counters, 0, (params.maximum_depth + 2) * sizeof(BounceCounters),
+                            stream));
+    const unsigned blocks = (init.count + 127) / 128;
+    if (init.kind == kInitRays) {
+        init_rays_kernel<<<blocks, 128, 0, stream>>>(a, init);
+    } else {
+        init_camera_kernel<<<blocks, 128, 0, stream>>>(a, init);
+    }
+    const LaunchShape& shape = launch_shape();
+    const bool         media = scene.d.medium_count > 0;
+    KernelTiming&      timing = kernel_timing();
+    bool               timed  = false;
+    {
+        std::lock_guard<std::mutex> lock(timing.mutex);
+        timed = timing.enabled;
+    }
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
+    unsigned long long before[2] = {0, 0};
+    if (timed) {
+        MR_CUDA(cudaMemcpyAsync(before, ws.queues.stats + kStatExtendBounds, sizeof(before),
+                                cudaMemcpyDeviceToHost, stream));
+        MR_CUDA(cudaStreamSynchronize(stream));
+    }
+    for (uint32_t bounce = 0; bounce <= params.maximum_depth; ++bounce) {
+        a.bounce = bounce;
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        if (timed) {
+            cudaEventCreate(&e0);
+            cudaEventCreate(&e1);
+            cudaEventRecord(e0, stream);
+        }
+        if (media) {
+            extend_kernel<true><<<shape.extend_blocks[1], 128, 0, stream>>>(a);
+        } else {
+            extend_kernel<false><<<shape.extend_blocks[0], 128, 0, stream>>>(a);
+        }
+        if (timed) {
+            cudaEventRecord(e1, stream);
+            events.emplace_back(e0, e1);
+        }
+        shade_kernel<<<shape.shade_blocks, 128, 0, stream>>>(a);
+        a.occluded_out = bounce == 0 && init.capture ? init.capture->occluded : nullptr;
+        if (media) {
+            shadow_kernel<true><<<shape.shadow_blocks[1], 128, 0, stream>>>(a);
+        } else {
+            shadow_kernel<false><<<shape.shadow_blocks[0], 128, 0, stream>>>(a);
+        }
+        if (bounce == 0 && init.capture) {
+            capture_shadow_kernel<<<(init.count + 127) / 128, 128, 0, stream>>>(a, init.capture->rays,
+                                                                                init.capture->has_shadow);
+        }
+        a.occluded_out = nullptr;
+    }
+    MR_CUDA(cudaGetLastError());
+    if (timed) {
+        unsigned long long after[2] = {0, 0};
+        MR_CUDA(cudaMemcpyAsync(after, ws.queues.stats + kStatExtendBounds, sizeof(after),
+                                cudaMemcpyDeviceToHost, stream));
+        MR_CUDA(cudaStreamSynchronize(stream));
+        double seconds = 0;
+        for (auto& [e0, e1] : events) {
+            float ms = 0;
+            cudaEventElapsedTime(&ms, e0, e1);
+            seconds += ms * 1e-3;
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+        }
+        std::lock_guard<std::mutex> lock(timing.mutex);
+        timing.launches += events.size();
+        timing.seconds += seconds;
+        timing.counted.bounds_tests += after[0] - before[0];
+        timing.counted.triangle_tests += after[1] - before[1];
+    }
+}
+
+void render_tile(const Scene& scene, const IntegratorParams& params, const mr_render_settings& render,
+                 uint32_t x0, uint32_t y0, uint32_t w, uint32_t h, uint32_t s0, uint32_t ns,
+                 float4* accumulator, Workspace& ws, cudaStream_t stream) {
+    const size_t area = static_cast<size_t>(w) * h;
+    if (area == 0 || ns == 0) {
+        return;
+    }
+    // Split the sample range (and, for huge tiles, the rows) into waves that fit the workspace.
+    const uint32_t rows_per_wave =
+        area <= ws.capacity ? h : static_cast<uint32_t>(std::max<size_t>(1, ws.capacity / w));
+    for (uint32_t ry = 0; ry < h; ry += rows_per_wave) {
+        const uint32_t hh      = std::min(rows_per_wave, h - ry);
+        const size_t   a       = static_cast<size_t>(w) * hh;
+        const uint32_t per     = static_cast<uint32_t>(std::max<size_t>(1, std::min<size_t>(ns, ws.capacity / a)));
+        for (uint32_t s = 0; s < ns; s += per) {
+            WaveInit init{};
+            init.kind   = kInitCamera;
+            init.x0     = x0;
+            init.y0     = y0 + ry;
+            init.w      = w;
+            init.h      = hh;
+            init.s0     = s0 + s;
+            init.ns     = std::min(per, ns - s);
+            init.width  = static_cast<uint32_t>(render.width);
+            init.height = static_cast<uint32_t>(render.height);
+            init.seed   = render.seed;
+            init.count  = static_cast<uint32_t>(a * init.ns);
+            Engine::run_wave(scene, params, init, ws, stream);
+            resolve_kernel<<<static_cast<unsigned>((a + 255) / 256), 256, 0, stream>>>(
+                ws.state.radiance, init.x0, init.y0, w, hh, init.ns, init.width, accumulator,
+                ws.queues.error);
+        }
+    }
+    MR_CUDA(cudaGetLastError());
+}
+
+void render_frame(const Scene& scene, const IntegratorParams& params, const mr_render_settings& render,
+                  float* device_rgb, cudaStream_t stream, mr_path_statistics* statistics,
+                  size_t max_paths) {
+    const size_t pixels   = static_cast<size_t>(render.width) * render.height;
+    const size_t total    = pixels * render.samples_per_pixel;
+    const size_t capacity = std::min(total, max_paths ? max_paths : (size_t(1) << 23));
+    auto         ws       = acquire_workspace(capacity, params.maximum_depth + 1, pixels);
+    reset_statistics(*ws, stream);
+    MR_CUDA(cudaMemsetAsync(ws->accumulator, 0, 2 * pixels * sizeof(float4), stream));
+    render_tile(scene, params, render, 0, 0, static_cast<uint32_t>(render.width),
+                static_cast<uint32_t>(render.height), 0, render.samples_per_pixel, ws->accumulator,
+                *ws, stream);
+    finalize_kernel<<<static_cast<unsigned>((pixels + 255) / 256), 256, 0, stream>>>(
+        ws->accumulator, pixels, render.samples_per_pixel, device_rgb, ws->queues.error);
+    MR_CUDA(cudaGetLastError());
+    unsigned error = 0;
+    read_statistics(*ws, stream, statistics, &error);
+    release_workspace(ws);
+    std::string message;
+    const mr_status status = error_status(error, message);
+    if (status != MR_OK) {
+        fail(status, message);
+    }
+}
+
+// Per-path radiance of an explicit wave (trace_paths / sample_pixels).
+void copy_path_radiance(Workspace& ws, uint32_t count, float* device_out, cudaStream_t stream) {
+    copy_radiance_kernel<<<(count + 255) / 256, 256, 0, stream>>>(ws.state.radiance, count, device_out);
+    MR_CUDA(cudaGetLastError());
+}
+
+}  // namespace mr

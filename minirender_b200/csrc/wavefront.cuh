@@ -1,0 +1,156 @@
+// wavefront.cuh — path state, queues and the wavefront driver interface.
+#pragma once
+
+#include <mutex>
+#include <vector>
+
+#include "scene.cuh"
+
+namespace mr {
+
+// Material bins of the extension result: paths are shaded bin by bin (sorted by material).
+enum Bin : int {
+    kBinMiss       = 0,
+    kBinDiffuse    = 1,
+    kBinConductor  = 2,
+    kBinMirror     = 3,
+    kBinDielectric = 4,
+    kBinMedium     = 5,
+    kBinCount      = 6,
+};
+
+struct BounceCounters {
+    uint32_t ext;                 // paths entering this bounce
+    uint32_t bins[kBinCount];
+    uint32_t shadow;
+    uint32_t work_extend;
+    uint32_t work_shadow;
+    uint32_t pad[6];
+};
+
+enum Stat : int {
+    kStatPaths = 0,
+    kStatShadowRays,
+    kStatScattering,
+    kStatRoulette,
+    kStatMedium,
+    kStatExtendBounds,
+    kStatExtendTriangles,
+    kStatShadowBounds,
+    kStatShadowTriangles,
+    kStatCount
+};
+
+struct IntegratorParams {
+    uint32_t mode;
+    uint32_t maximum_depth;
+    uint32_t russian_roulette;
+    uint32_t roulette_depth;
+};
+
+// Structure-of-arrays path state of `capacity` paths (one 16-byte record per field).
+struct PathState {
+    ulonglong2* rng;       // PCG state, increment
+    float4*     beta;      // throughput, eta scale
+    float4*     radiance;  // accumulated radiance
+    float4*     prev;      // previous scattering vertex, previous pdf
+    uint32_t*   flags;     // bit 0: previous event was delta
+    float4*     ray_o;     // origin, interval minimum
+    float4*     ray_d;     // direction, interval maximum
+    float4*     hit;       // distance, barycentrics (medium: distance, anisotropy)
+    uint32_t*   hit_slot;  // triangle slot, kNone on a miss
+    float4*     shadow_o;  // shadow origin, segment limit
+    float4*     shadow_d;  // shadow direction
+    float4*     shadow_c;  // unoccluded contribution
+};
+
+struct Queues {
+    uint32_t*       ext[2];
+    uint32_t*       bins;    // kBinCount * capacity
+    uint32_t*       shadow;
+    BounceCounters* counters;  // maximum_depth + 2 entries
+    unsigned long long* stats;  // kStatCount
+    unsigned*           error;
+};
+
+// Device workspace for `capacity` concurrent paths; pooled and reused across renders.
+struct Workspace {
+    size_t    capacity     = 0;
+    uint32_t  max_bounces  = 0;
+    void*     memory       = nullptr;
+    size_t    bytes        = 0;
+    PathState state{};
+    Queues    queues{};
+    float4*   accumulator  = nullptr;  // Kahan sum per pixel (sum, compensation) of a frame
+    size_t    pixels       = 0;
+    ~Workspace();
+};
+
+// Diagnostics: first-bounce shadow rays (2 float4 per path), a flag per path that one was
+// traced, and its occlusion result (device buffers of the wave's path count).
+struct ShadowCapture {
+    float4*  rays;
+    uint8_t* has_shadow;
+    uint8_t* occluded;
+};
+
+// How the paths of one wave start.
+enum InitKind : int { kInitCamera = 0, kInitPixelList = 1, kInitRays = 2 };
+
+struct WaveInit {
+    InitKind        kind;
+    // camera waves: pixel rectangle x0..x0+w, y0..y0+h of a width x height image, samples
+    // s0..s0+ns, sample-major slots.
+    uint32_t        x0, y0, w, h;
+    uint32_t        s0, ns;
+    uint32_t        width, height;
+    uint64_t        seed;
+    // pixel lists / explicit rays
+    const uint32_t* pixels;   // x, y pairs (device)
+    const uint64_t* samples;  // (device)
+    const float4*   rays;     // origin+min, direction+max pairs (device)
+    const uint64_t* keys;     // seed, pixel, sample triples (device)
+    uint32_t        count;
+    float4*         camera_rays_out;  // optional (device), 2 float4 per path
+    ShadowCapture*  capture;          // optional diagnostics (host struct of device pointers)
+};
+
+class Engine {
+  public:
+    // Renders one wave on `stream`: initialises `count` paths, runs up to maximum_depth + 1
+    // bounces. Path radiance stays in ws.state.radiance (slot order).
+    static void run_wave(const Scene& scene, const IntegratorParams& params, const WaveInit& init,
+                         Workspace& ws, cudaStream_t stream);
+};
+
+// Workspace pool (per device).
+std::shared_ptr<Workspace> acquire_workspace(size_t capacity, uint32_t max_bounces, size_t pixels);
+void                       release_workspace(std::shared_ptr<Workspace> ws);
+
+// Kernel timing for roofline figures (nearest-hit traversal launches).
+struct KernelTiming {
+    std::mutex         mutex;
+    bool               enabled  = false;
+    uint64_t           launches = 0;
+    double             seconds  = 0;
+    mr_trace_statistics counted{};
+};
+KernelTiming& kernel_timing();
+
+// Frame render into a device image (width*height*3 floats) — used by mr_render(_device) and the
+// session. Statistics (optional) are read back after the frame.
+void render_frame(const Scene& scene, const IntegratorParams& params, const mr_render_settings& render,
+                  float* device_rgb, cudaStream_t stream, mr_path_statistics* statistics,
+                  size_t max_paths = 0);
+
+// Accumulates the samples [s0, s0+ns) of a pixel rectangle into a caller-owned Kahan
+// accumulator (float4 sum + float4 compensation per pixel of the full image).
+void render_tile(const Scene& scene, const IntegratorParams& params, const mr_render_settings& render,
+                 uint32_t x0, uint32_t y0, uint32_t w, uint32_t h, uint32_t s0, uint32_t ns,
+                 float4* accumulator, Workspace& ws, cudaStream_t stream);
+
+void read_statistics(Workspace& ws, cudaStream_t stream, mr_path_statistics* out, unsigned* error);
+void reset_statistics(Workspace& ws, cudaStream_t stream);
+mr_status error_status(unsigned error, std::string& message);
+
+}  // namespace mr

@@ -1,0 +1,417 @@
+"""GPU parity: the CUDA path tracer (through the C ABI) against the FP64 CPU oracle.
+
+Bars (all stated here):
+  * hit records: with the oracle's (reference-algorithm) BVH imported, primary camera rays and the
+    integrator's own shadow rays give the oracle's hit/miss and primitive id, except documented
+    classes: t-ties (the two candidate primitives' FP64 distances within 4 FP32 ulps) and
+    edge grazes (the FP64 ray passes within 1e-5 relative of the chosen triangle's edge);
+  * analytic integrator cases of tests/path_tests.cpp hold in FP32 (tolerances below);
+  * images at equal seeds: per-pixel |gpu - cpu| <= 2e-3 * max(cpu, 0.05 * mean) for at least
+    99% of pixels, and the image means agree within 0.5%;
+  * the GPU binned-SAH tree costs within 2% of the reference builder's tree, and gives the same
+    nearest hits as the imported reference tree.
+"""
+
+import math
+
+import numpy as np
+import pytest
+
+from minirender_b200 import scene as sc
+
+pytestmark = pytest.mark.gpu
+
+from tests.test_oracle_golden import (direct_doc, emitter_doc, floor_doc, lcg_rays,  # noqa: E402
+                                      sampler_doubles, studio_cubes, triangle_doc)
+
+
+@pytest.fixture(scope="module")
+def api():
+    from minirender_b200 import api as a
+    return a
+
+
+def small_spheres(count=12, seed=3):
+    doc = sc.sphere_field(count, 6.0, seed, subdivisions=2)
+    doc.camera = sc.Camera(position=(0.0, 3.0, 9.0), target=(0.0, 2.5, 0.0), aperture_radius=0.05,
+                           focus_distance=8.0, vertical_fov_degrees=45.0)
+    return doc
+
+
+def gpu_and_oracle(api, oracle, doc, imported=True, settings=None):
+    snap = doc.snapshot()
+    o = oracle.OracleScene(snap, settings)
+    bvh = o.export_bvh() if imported else None
+    g = api.Scene(snap, bvh)
+    return g, o, snap
+
+
+def classify_mismatch(tris, o, d, t_cpu, prim_cpu, prim_gpu):
+    """Returns 'tie' when both primitives are hit at FP64 distances within 4 FP32 ulps, or
+    'graze' when the ray passes within 1e-5 (relative) of an edge of either triangle."""
+    def mt(tri):
+        v0, v1, v2 = (tri[k].astype(np.float64) for k in range(3))
+        e1, e2 = v1 - v0, v2 - v0
+        p = np.cross(d, e2)
+        det = e1 @ p
+        if abs(det) < 1e-300:
+            return None, 0.0
+        off = o - v0
+        u = (off @ p) / det
+        q = np.cross(off, e1)
+        v = (d @ q) / det
+        t = (e2 @ q) / det
+        return t, min(u, v, 1 - u - v)
+    ts, margins = [], []
+    for prim in (prim_cpu, prim_gpu):
+        if prim is None:
+            continue
+        t, m = mt(tris[prim])
+        ts.append(t)
+        margins.append(m)
+    if len(ts) == 2 and ts[0] is not None and ts[1] is not None:
+        if abs(ts[0] - ts[1]) <= 4 * np.spacing(np.float32(max(abs(ts[0]), 1e-30))):
+            return "tie"
+    if any(abs(m) <= 1e-5 for m in margins):
+        return "graze"
+    return "unexplained"
+
+
+def compare_hits(g_hits, c_hits, tris, origins, dirs):
+    classes = {"tie": 0, "graze": 0, "unexplained": 0}
+    for i in range(len(g_hits)):
+        ghit = g_hits["primitive"][i] != 0xFFFFFFFF
+        chit = c_hits[i, 0] == 1
+        gp = int(g_hits["primitive"][i]) if ghit else None
+        cp = int(c_hits[i, 4]) if chit else None
+        if ghit == chit and gp == cp:
+            continue
+        cls = classify_mismatch(tris, origins[i].astype(np.float64), dirs[i].astype(np.float64),
+                                c_hits[i, 1], cp, gp)
+        classes[cls] += 1
+    return classes
+
+
+# ---- camera rays and primary hit records ----
+
+@pytest.mark.parametrize("name", ["cornell", "spheres"])
+def test_primary_hit_records_match_oracle(api, oracle, name):
+    doc = sc.cornell_box() if name == "cornell" else small_spheres()
+    g, o, snap = gpu_and_oracle(api, oracle, doc)
+    w, h, spp = 64, 48, 4
+    render = api.RenderSettings(w, h, spp, 7)
+    xs, ys = np.meshgrid(np.arange(w), np.arange(h))
+    pixels = np.repeat(np.stack([xs.ravel(), ys.ravel()], 1), spp, axis=0)
+    samples = np.tile(np.arange(spp), w * h)
+    tracer = api.PathTracer(g, api.IntegratorSettings("mis", 1, False, 3))
+    _, _, rays = tracer.sample_pixels(render, pixels, samples, want_rays=True)
+    # camera rays against the oracle's FP64 camera
+    _, _, crays = o.sample_pixels(api.RenderSettings(w, h, spp, 7).c(), pixels, samples,
+                                  want_rays=True)
+    assert np.max(np.abs(rays[:, 3:6] - crays[:, 3:6])) < 2e-6
+    assert np.max(np.abs(rays[:, 0:3] - crays[:, 0:3])) < 1e-5
+    # hit records for the GPU's own FP32 rays, traced by both
+    g_hits, _ = g.intersect(rays[:, 0:3], rays[:, 3:6], rays[:, 6], rays[:, 7])
+    c_hits, _ = o.intersect(rays[:, 0:3].astype(np.float64), rays[:, 3:6].astype(np.float64),
+                            rays[:, 6].astype(np.float64), rays[:, 7].astype(np.float64))
+    classes = compare_hits(g_hits, c_hits, o.primitives(), rays[:, 0:3], rays[:, 3:6])
+    assert classes["unexplained"] == 0, classes
+    assert classes["tie"] + classes["graze"] <= max(2, len(rays) // 5000), classes
+
+
+@pytest.mark.parametrize("name", ["cornell", "spheres"])
+def test_shadow_hit_records_match_oracle(api, oracle, name):
+    doc = sc.cornell_box() if name == "cornell" else small_spheres()
+    g, o, snap = gpu_and_oracle(api, oracle, doc)
+    w, h, spp = 64, 48, 2
+    xs, ys = np.meshgrid(np.arange(w), np.arange(h))
+    pixels = np.repeat(np.stack([xs.ravel(), ys.ravel()], 1), spp, axis=0)
+    samples = np.tile(np.arange(spp), w * h)
+    tracer = api.PathTracer(g, api.IntegratorSettings("mis", 4, False, 3))
+    rays, has, occ = tracer.capture_shadow_rays(api.RenderSettings(w, h, spp, 11), pixels, samples)
+    assert has.sum() > 1000
+    r = rays[has]
+    c_occ, _ = o.occluded(r[:, 0:3].astype(np.float64), r[:, 3:6].astype(np.float64),
+                          r[:, 6].astype(np.float64), r[:, 7].astype(np.float64))
+    mismatches = int(np.sum(c_occ != occ[has]))
+    assert mismatches <= max(1, int(has.sum()) // 5000), mismatches
+
+
+def test_lcg_rays_against_brute_force(api, oracle):
+    # tests/intersection_tests.cpp:264-311 on the GPU, with the GPU-built BVH.
+    from tests.test_oracle_golden import brute_force
+    snap = studio_cubes().snapshot()
+    g = api.Scene(snap)
+    o = oracle.OracleScene(snap)
+    tris = o.primitives()
+    mirrored = np.repeat([np.linalg.det(m[:3, :3].astype(np.float64)) < 0 for m, _ in snap.matrices], 12)
+    origins, dirs = lcg_rays()
+    tmax = np.where(np.arange(4000) % 2 == 1, 100.0, 3.0).astype(np.float32)
+    hits, stats = g.intersect(origins, dirs, 1e-5, tmax)
+    occ, _ = g.occluded(origins, dirs, 1e-5, tmax)
+    found = 0
+    for i in range(4000):
+        ref = brute_force(tris, (np.ones(len(tris), bool), mirrored), origins[i].astype(np.float64),
+                          dirs[i].astype(np.float64), 1e-5, float(tmax[i]))
+        ghit = hits["primitive"][i] != 0xFFFFFFFF
+        assert ghit == (ref is not None)
+        assert occ[i] == (ref is not None)
+        if ref is not None:
+            found += 1
+            assert hits["distance"][i] == pytest.approx(ref[1], rel=2e-6, abs=1e-6)
+            assert int(hits["primitive"][i]) == ref[0]
+    assert found > 300
+    assert stats["triangle_tests"] < len(tris) * 4000
+
+
+def test_coincident_triangles_and_any_hit_early_exit(api):
+    doc = triangle_doc()
+    for _ in range(255):
+        doc.objects.append(sc.SceneObject(0, 0))
+    snap = doc.snapshot()
+    from oracle import pyoracle
+    o = pyoracle.OracleScene(snap)
+    g = api.Scene(snap, o.export_bvh())
+    hits, nearest = g.intersect([[0.25, 0.25, 2]], [[0, 0, -1]])
+    occ, shadow = g.occluded([[0.25, 0.25, 2]], [[0, 0, -1]])
+    assert hits["instance"][0] == 0 and occ[0]
+    assert nearest["triangle_tests"] == 256 and shadow["triangle_tests"] == 1
+    assert not g.occluded([[0.25, 0.25, 2]], [[0, 0, -1]], 0, 1.9)[0][0]
+
+
+def test_single_sided_culling(api):
+    for double_sided in (False, True):
+        g = api.Scene(triangle_doc(double_sided=double_sided).snapshot())
+        front, _ = g.intersect([[0.2, 0.2, 2]], [[0, 0, -1]])
+        back, _ = g.intersect([[0.2, 0.2, -2]], [[0, 0, 1]])
+        assert front["primitive"][0] == 0 and front["front_face"][0] == 1
+        assert (back["primitive"][0] == 0) == double_sided
+
+
+# ---- analytic integrator cases (tests/path_tests.cpp) in FP32 ----
+
+def estimate(tracer, count, seed, origin=(0, 1, 0), direction=(0, -1, 0), interval=(0, 10000)):
+    keys = np.zeros((count, 3), np.uint64)
+    keys[:, 0] = seed
+    keys[:, 2] = np.arange(count)
+    rad, stats = tracer.trace([origin] * count, [direction] * count, interval[0], interval[1], keys)
+    x = rad[:, 0].astype(np.float64)
+    return x.mean(), x.std(ddof=1) / math.sqrt(count), stats
+
+
+@pytest.mark.parametrize("mode", ["bsdf", "light", "mis"])
+def test_diffuse_constant_environment(api, mode):
+    t = api.PathTracer(floor_doc().snapshot(), api.IntegratorSettings(mode, 1, False, 3))
+    mean, se, _ = estimate(t, 8192, 81)
+    assert abs(mean - 0.6) < 5 * se + 1e-6
+
+
+@pytest.mark.parametrize("mode", ["bsdf", "light", "mis"])
+def test_directional_light_exact(api, mode):
+    doc = floor_doc()
+    doc.environment = (0.0, 0.0, 0.0)
+    irradiance = float(np.float32(math.pi))
+    doc.directional_lights.append(sc.DirectionalLight((0, -1, 0), (1, 1, 1), irradiance))
+    t = api.PathTracer(doc.snapshot(), api.IntegratorSettings(mode, 1, False, 3))
+    mean, _, _ = estimate(t, 32, 3)
+    assert mean == pytest.approx(0.6 * irradiance / math.pi, rel=2e-6)
+
+
+@pytest.mark.parametrize("mode", ["bsdf", "light", "mis"])
+def test_mirror_and_glass_exact(api, mode):
+    t = api.PathTracer(floor_doc("mirror", 0.7).snapshot(), api.IntegratorSettings(mode, 2, False, 3))
+    assert estimate(t, 128, 9)[0] == pytest.approx(0.7, rel=1e-6)
+    glass = floor_doc("dielectric", 1.0)
+    glass.objects.append(sc.SceneObject(0, 0, sc.Transform((0.0, -1.0, 0.0), (180.0, 0.0, 0.0),
+                                                           (4.0, 1.0, 4.0))))
+    t = api.PathTracer(glass.snapshot(), api.IntegratorSettings(mode, 12, False, 3))
+    assert estimate(t, 1024, 125)[0] == pytest.approx(1.0, rel=1e-5)
+
+
+def test_depth_zero_returns_emission(api):
+    doc = floor_doc()
+    doc.environment = (0.0, 0.0, 0.0)
+    doc.materials[0].emission = (8.0, 2.0, 0.5)
+    t = api.PathTracer(doc.snapshot(), api.IntegratorSettings("mis", 0, False, 3))
+    rad, stats = t.trace([[0, 1, 0]], [[0, -1, 0]], 0, 100, np.array([[9, 0, 0]], np.uint64))
+    assert rad[0].tolist() == [8, 2, 0.5]
+    assert stats["scattering_events"] == 0 and stats["shadow_rays"] == 0
+
+
+def test_russian_roulette_mean(api):
+    doc = floor_doc("diffuse", 0.5)
+    doc.environment = (0.0, 0.0, 0.0)
+    doc.materials[0].emission = (1.0, 1.0, 1.0)
+    doc.objects[0].transform = sc.Transform(scale=(1000.0, 1.0, 1000.0))
+    doc.objects.append(sc.SceneObject(0, 0, sc.Transform((0.0, 2.0, 0.0), (0, 0, 0),
+                                                         (1000.0, 1.0, 1000.0))))
+    snap = doc.snapshot()
+    m0, e0, s0 = estimate(api.PathTracer(snap, api.IntegratorSettings("bsdf", 8, False, 1)), 4096, 13)
+    m1, e1, s1 = estimate(api.PathTracer(snap, api.IntegratorSettings("bsdf", 8, True, 1)), 16384, 14)
+    assert abs(m1 - m0) < 5 * math.hypot(e0, e1) + 0.002
+    assert m0 == pytest.approx(2 - 1 / 256, abs=0.003)
+    assert s1["roulette_terminations"] > 0
+
+
+def test_false_endpoint_occlusions_fp32(api, oracle):
+    # tests/path_tests.cpp:103-120 through the integrator's own FP32 shadow segments: a receiver
+    # facing a lone emitter sees it on every light sample, so no NEE sample may be occluded by
+    # the emitter's own triangle at the far end of the segment.
+    doc = emitter_doc()
+    doc.materials.append(sc.Material(base_color=(0.5, 0.5, 0.5)))
+    doc.meshes.append(sc.quad_mesh([(-5, -5, 5), (5, -5, 5), (5, 5, 5), (-5, 5, 5)], (0, 0, -1)))
+    doc.objects.append(sc.SceneObject(1, 1))
+    t = api.PathTracer(doc.snapshot(), api.IntegratorSettings("light", 1, False, 3))
+    keys = np.zeros((1000, 3), np.uint64)
+    keys[:, 0] = 171
+    keys[:, 2] = np.arange(1000)
+    rad, stats = t.trace([[0.5, 0.25, 4.0]] * 1000, [[0, 0, 1]] * 1000, 0, 100, keys)
+    assert stats["shadow_rays"] == 1000
+    o = oracle.OracleScene(doc.snapshot(), oracle.integrator("light", 1, False, 3))
+    ref, _ = o.trace_paths([[0.5, 0.25, 4.0]] * 1000, [[0, 0, 1]] * 1000, 0, 100, keys)
+    assert np.all(ref[:, 0] > 0)
+    assert np.sum(rad[:, 0] == 0) == 0
+    assert np.allclose(rad, ref, rtol=1e-4, atol=1e-7)
+
+
+def test_blocker_in_front_and_behind_light(api):
+    doc = direct_doc(False)
+    clear = api.PathTracer(doc.snapshot(), api.IntegratorSettings("light", 1, False, 3))
+    doc.materials.append(sc.Material(base_color=(0.0, 0.0, 0.0)))
+    blocker = sc.SceneObject(0, 2, sc.Transform((0.0, 1.0, 0.0), (0, 0, 0), (4.0, 1.0, 4.0)))
+    doc.objects.append(blocker)
+    blocked = api.PathTracer(doc.snapshot(), api.IntegratorSettings("light", 1, False, 3))
+    blocker.transform = sc.Transform((0.0, 3.0, 0.0), (0, 0, 0), (4.0, 1.0, 4.0))
+    behind = api.PathTracer(doc.snapshot(), api.IntegratorSettings("light", 1, False, 3))
+    keys = np.zeros((256, 3), np.uint64)
+    keys[:, 0] = 79
+    keys[:, 2] = np.arange(256)
+    args = ([[0, 0.5, 0]] * 256, [[0, -1, 0]] * 256, 0, np.inf, keys)
+    a, _ = clear.trace(*args)
+    b, _ = blocked.trace(*args)
+    c, _ = behind.trace(*args)
+    assert np.all(a[:, 0] > 0) and np.all(b == 0)
+    assert np.max(np.abs(c - a)) == 0
+
+
+def test_translation_invariance_fp32(api):
+    doc = direct_doc(False)
+    original = api.PathTracer(doc.snapshot(), api.IntegratorSettings("light", 1, False, 3))
+    for obj in doc.objects:
+        t = obj.transform
+        obj.transform = sc.Transform(tuple(np.float32(v) * np.float32(128) + np.float32(1e8)
+                                           for v in t.translation), t.rotation_degrees,
+                                     tuple(np.float32(v) * np.float32(128) for v in t.scale))
+    moved = api.PathTracer(doc.snapshot(), api.IntegratorSettings("light", 1, False, 3))
+    keys = np.zeros((512, 3), np.uint64)
+    keys[:, 0] = 5
+    keys[:, 2] = np.arange(512)
+    a, _ = original.trace([[0, 1, 0]] * 512, [[0, -1, 0]] * 512, 0, np.inf, keys)
+    b, _ = moved.trace([[1e8, 1e8 + 128, 1e8]] * 512, [[0, -1, 0]] * 512, 0, np.inf, keys)
+    assert np.all(b[:, 0] > 0)
+    assert np.allclose(a, b, rtol=2e-3, atol=1e-6)
+
+
+# ---- images at equal seeds ----
+
+@pytest.mark.parametrize("name", ["cornell", "spheres"])
+def test_image_matches_oracle_at_equal_seeds(api, oracle, name):
+    doc = sc.cornell_box() if name == "cornell" else small_spheres()
+    settings = api.IntegratorSettings("mis", 8, True, 3)
+    g, o, snap = gpu_and_oracle(api, oracle, doc, settings=oracle.integrator("mis", 8, True, 3))
+    render = api.RenderSettings(96, 72, 8, 1)
+    tracer = api.PathTracer(g, settings)
+    gpu, gstats = tracer.render(render)
+    cpu, cstats = o.render(render.c())
+    scale = max(cpu.mean(), 1e-6)
+    tol = 2e-3 * np.maximum(cpu, 0.05 * scale)
+    ok = np.all(np.abs(gpu - cpu) <= tol, axis=2)
+    assert ok.mean() >= 0.99, ok.mean()
+    assert gpu.mean() == pytest.approx(cpu.mean(), rel=5e-3)
+    assert gstats["paths"] == cstats["paths"] == 96 * 72 * 8
+    # path statistics agree closely (same streams, same decisions except rare FP32 flips)
+    for key in ("shadow_rays", "scattering_events", "roulette_terminations"):
+        assert gstats[key] == pytest.approx(cstats[key], rel=2e-3)
+
+
+def test_render_is_deterministic_and_session_bitwise_equal(api):
+    g = api.Scene(sc.cornell_box().snapshot())
+    tracer = api.PathTracer(g, api.IntegratorSettings("mis", 8, True, 3))
+    render = api.RenderSettings(64, 48, 9, 5)
+    a, _ = tracer.render(render)
+    b, _ = tracer.render(render)
+    assert np.array_equal(a, b)
+    session = api.RenderSession()
+    for batch in (1, 4, 9):
+        session.start(g, render, api.IntegratorSettings("mis", 8, True, 3),
+                      api.SessionSettings(0, 16, batch))
+        assert session.wait_for(60000)
+        session.wait()
+        p = session.progress()
+        assert p["state"] == "completed", p
+        assert p["recorded_samples"] == 64 * 48 * 9
+        assert p["completed_pixels"] == 64 * 48
+        assert np.array_equal(session.result(), a)
+        img, info = session.preview(0)
+        assert np.array_equal(img, a)
+        small, info = session.preview(8)
+        assert small.shape[0] <= 8 and small.shape[1] <= 8
+    assert session.progress()["job_id"] == 3
+    session.close()
+
+
+def test_session_pause_resume_cancel(api):
+    g = api.Scene(sc.cornell_box().snapshot())
+    session = api.RenderSession()
+    session.start(g, api.RenderSettings(64, 64, 100000, 3), api.IntegratorSettings(),
+                  api.SessionSettings(0, 16, 1))
+    import time
+    deadline = time.time() + 30
+    while session.progress()["recorded_samples"] == 0 and time.time() < deadline:
+        time.sleep(0.005)
+    with pytest.raises(Exception):
+        session.start(g, api.RenderSettings(8, 8, 1, 1))
+    assert session.pause()
+    while session.progress()["state"] != "paused" and time.time() < deadline:
+        time.sleep(0.005)
+    count = session.progress()["recorded_samples"]
+    time.sleep(0.05)
+    assert session.progress()["recorded_samples"] == count
+    for _ in range(5):
+        assert session.resume()
+        assert session.pause()
+        while session.progress()["state"] != "paused" and time.time() < deadline:
+            time.sleep(0.005)
+    session.cancel()
+    assert session.wait_for(10000)
+    session.wait()
+    assert session.progress()["state"] == "cancelled"
+    assert session.result() is None
+    session.close()
+
+
+# ---- GPU binned-SAH builder ----
+
+@pytest.mark.parametrize("name", ["cornell", "spheres", "cubes"])
+def test_gpu_builder_sah_within_two_percent(api, oracle, name):
+    doc = {"cornell": sc.cornell_box, "spheres": lambda: sc.sphere_field(40, 10.0, 9, 3),
+           "cubes": studio_cubes}[name]()
+    snap = doc.snapshot()
+    o = oracle.OracleScene(snap)
+    built = api.Scene(snap)
+    imported = api.Scene(snap, o.export_bvh())
+    ref_cost = o.sah_cost()
+    assert built.sah_cost() == pytest.approx(ref_cost, rel=0.02)
+    assert imported.sah_cost() == pytest.approx(ref_cost, rel=1e-9)
+    st = built.statistics()
+    assert st["triangles"] == snap.triangle_count and st["maximum_depth"] <= 48
+    # same nearest hits whichever tree is used
+    rng = np.random.default_rng(1)
+    origins = rng.uniform(-3, 3, (20000, 3)).astype(np.float32) + np.float32([0, 3, 8])
+    targets = rng.uniform(-3, 3, (20000, 3)).astype(np.float32) + np.float32([0, 2, 0])
+    d = targets - origins
+    d = (d / np.linalg.norm(d, axis=1, keepdims=True)).astype(np.float32)
+    a, _ = built.intersect(origins, d, 0, np.inf)
+    b, _ = imported.intersect(origins, d, 0, np.inf)
+    assert np.array_equal(a["primitive"], b["primitive"])
+    assert np.array_equal(a["distance"], b["distance"])
