@@ -16,6 +16,7 @@
 namespace mr {
 
 constexpr int      kStackSize  = 64;  // trees are at most 48 levels deep (bvh.cpp:126)
+constexpr uint32_t kMaxVisits  = 1u << 24;  // node visits per ray before the query gives up
 
 struct RayQuery {
     f3    o, d;
@@ -161,9 +162,14 @@ __device__ __forceinline__ TraceResult trace(const DeviceScene& s, const RayQuer
     }
     int2  stack[kStackSize];
     int   sp        = 0;
-    int   node      = s.root;
-    float node_tmin = root_enter;
+    int      node      = s.root;
+    float    node_tmin = root_enter;
+    uint32_t visits    = 0;
     while (true) {
+        if (++visits > kMaxVisits) {  // only a malformed tree can get here
+            error |= kErrorStack;
+            return result;
+        }
         if (node >= 0) {
             const float4* n  = s.nodes + 4 * static_cast<size_t>(node);
             const float4  lxy = __ldg(n + 0);
