@@ -8,10 +8,3 @@
 from . import scene  # noqa: F401
 
 __all__ = ["scene", "api"]
-
-
-def __getattr__(name):
-    if name == "api":
-        from . import api
-        return api
-    raise AttributeError(name)

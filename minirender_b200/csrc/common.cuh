@@ -27,6 +27,8 @@ enum ErrorBits : unsigned {
     kErrorOverflow = 2u,  // pixel above FLT_MAX (std::overflow_error)
     kErrorStack    = 4u,  // traversal stack exhausted (never for trees of depth <= 48)
     kErrorMedium   = 8u,  // zero mixture probability in free-flight sampling
+    kErrorVisits   = 16u, // a ray visited more nodes than any well-formed tree allows
+    kErrorRay      = 32u, // a ray with a nonfinite origin or direction reached traversal
 };
 
 struct f3 {

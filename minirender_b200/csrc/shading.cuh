@@ -423,7 +423,7 @@ __device__ __forceinline__ float environment_pdf(const DeviceScene& s) {  // lig
 }
 
 // The shadow segment of PathTracer::shadow_transmittance (path_tracer.cpp:259-284): both ends
-// offset by their error bounds, the far end pulled in by one ulp. Returns false when the
+// offset by their error bounds, the far end pulled in by one ulp and 2^-18 of its length. Returns false when the
 // segment has zero length (the reference returns zero transmittance without tracing).
 __device__ __forceinline__ bool shadow_segment(f3 origin, const LightSample& light, f3& direction,
                                                float& limit) {
@@ -438,7 +438,10 @@ __device__ __forceinline__ bool shadow_segment(f3 origin, const LightSample& lig
             return false;
         }
         direction = difference / limit;
-        limit     = nextafterf(limit, 0.0f);
+        // One ulp as in the reference, then 2^-18 of the length: the FP32 distance the triangle
+        // test computes for the light's own triangle carries an error of a few ulps of the
+        // segment length (not of the light point's coordinates, which set the offset above).
+        limit = nextafterf(limit, 0.0f) * 0.99999618530273437500f;  // 1 - 2^-18
     }
     return true;
 }

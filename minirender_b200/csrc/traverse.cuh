@@ -16,7 +16,7 @@
 namespace mr {
 
 constexpr int      kStackSize  = 64;  // trees are at most 48 levels deep (bvh.cpp:126)
-constexpr uint32_t kMaxVisits  = 1u << 24;  // node visits per ray before the query gives up
+constexpr uint32_t kMaxVisits  = 1u << 16;  // node visits per ray before the query gives up
 
 struct RayQuery {
     f3    o, d;
@@ -58,8 +58,8 @@ struct RayQuery {
     }
 };
 
-// Entry distance of one child box, or +inf when the slab intervals do not overlap within
-// [tmin, tmax]. `xy` = (lo.x, hi.x, lo.y, hi.y); (zlo, zhi) the z extent.
+// Entry distance of one child box, or NaN when the slab intervals do not overlap within
+// [tmin, tmax] (NaN compares false against every interval end, +inf would not for tmax = inf). `xy` = (lo.x, hi.x, lo.y, hi.y); (zlo, zhi) the z extent.
 __device__ __forceinline__ float slab_enter(const RayQuery& q, float4 xy, float zlo, float zhi,
                                             float tmin, float tmax) {
     const float nx = ((q.neg[0] ? xy.y : xy.x) - q.o.x) * q.inv_lo[0];
@@ -71,7 +71,7 @@ __device__ __forceinline__ float slab_enter(const RayQuery& q, float4 xy, float 
     // fmaxf/fminf ignore the NaN of 0 * inf (origin on the slab plane of a zero component).
     const float enter = fmaxf(fmaxf(tmin, nx), fmaxf(ny, nz));
     const float leave = fminf(fminf(tmax, fx), fminf(fy, fz));
-    return enter <= leave ? enter : __int_as_float(0x7f800000);
+    return enter <= leave ? enter : __int_as_float(0x7fffffff);
 }
 
 __device__ __forceinline__ float permuted(f3 v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
@@ -152,6 +152,10 @@ __device__ __forceinline__ TraceResult trace(const DeviceScene& s, const RayQuer
     if (!s.has_nodes) {
         return result;
     }
+    if (!(finite3(q.o) && finite3(q.d))) {
+        error |= kErrorRay;
+        return result;
+    }
     // The root's own box (src/render/bvh.cpp:331-334).
     counters.bounds++;
     const float root_enter =
@@ -167,7 +171,7 @@ __device__ __forceinline__ TraceResult trace(const DeviceScene& s, const RayQuer
     uint32_t visits    = 0;
     while (true) {
         if (++visits > kMaxVisits) {  // only a malformed tree can get here
-            error |= kErrorStack;
+            error |= kErrorVisits;
             return result;
         }
         if (node >= 0) {

@@ -773,6 +773,14 @@ mr_status error_status(unsigned error, std::string& message) {
         message = "Medium sample has zero mixture probability";
         return MR_RUNTIME_ERROR;
     }
+    if (error & kErrorRay) {
+        message = "A ray with a nonfinite origin or direction reached traversal";
+        return MR_RUNTIME_ERROR;
+    }
+    if (error & kErrorVisits) {
+        message = "BVH traversal exceeded its node-visit bound";
+        return MR_RUNTIME_ERROR;
+    }
     if (error & kErrorStack) {
         message = "BVH traversal stack exhausted";
         return MR_RUNTIME_ERROR;
