@@ -370,10 +370,12 @@ mr_status mr_display_image(const float* linear, uint64_t width, uint64_t height,
 
 /* Kernel timing for roofline figures: when enabled, the library records CUDA events around
  * every launch of the nearest-hit traversal kernel on its launching stream; `mr_kernel_timing`
- * returns the number of launches, their summed device time in seconds and the summed
- * bounds/triangle test counters of those launches. No reference counterpart. */
+ * returns the number of those launches, their summed device time in seconds, the summed
+ * bounds/triangle test counters of those launches, and the number of all kernels the library
+ * launched while timing was enabled. Enabling resets the figures. No reference counterpart. */
 mr_status mr_set_kernel_timing(int enabled);
-mr_status mr_kernel_timing(uint64_t* launches, double* seconds, mr_trace_statistics* counted);
+mr_status mr_kernel_timing(uint64_t* launches, double* seconds, mr_trace_statistics* counted,
+                           uint64_t* all_launches);
 
 /* ---- session ---------------------------------------------------------------------------- */
 

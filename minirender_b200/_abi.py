@@ -191,7 +191,8 @@ SIGNATURES = {
     "mr_display_image": (C.c_int, [P(C.c_float), C.c_uint64, C.c_uint64, C.c_double,
                                    P(C.c_float)]),
     "mr_set_kernel_timing": (C.c_int, [C.c_int]),
-    "mr_kernel_timing": (C.c_int, [P(C.c_uint64), P(C.c_double), P(TraceStatistics)]),
+    "mr_kernel_timing": (C.c_int, [P(C.c_uint64), P(C.c_double), P(TraceStatistics),
+                                   P(C.c_uint64)]),
     "mr_session_create": (C.c_int, [P(VP)]),
     "mr_session_destroy": (C.c_int, [VP]),
     "mr_session_start": (C.c_int, [VP, VP, P(RenderSettings), P(IntegratorSettings),

@@ -689,19 +689,22 @@ mr_status mr_set_kernel_timing(int enabled) {
         KernelTiming&               t = kernel_timing();
         std::lock_guard<std::mutex> lock(t.mutex);
         t.enabled  = enabled != 0;
+        t.all_launches = 0;
         t.launches = 0;
         t.seconds  = 0;
         t.counted  = {};
     });
 }
 
-mr_status mr_kernel_timing(uint64_t* launches, double* seconds, mr_trace_statistics* counted) {
+mr_status mr_kernel_timing(uint64_t* launches, double* seconds, mr_trace_statistics* counted,
+                           uint64_t* all_launches) {
     return guarded([&] {
         KernelTiming&               t = kernel_timing();
         std::lock_guard<std::mutex> lock(t.mutex);
         if (launches) *launches = t.launches;
         if (seconds) *seconds = t.seconds;
         if (counted) *counted = t.counted;
+        if (all_launches) *all_launches = t.all_launches.load();
     });
 }
 

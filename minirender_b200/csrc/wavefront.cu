@@ -816,10 +816,8 @@ void Engine::run_wave(const Scene& scene, const IntegratorParams& params, const 
     const bool         media = scene.d.medium_count > 0;
     KernelTiming&      timing = kernel_timing();
     bool               timed  = false;
-    {
-        std::lock_guard<std::mutex> lock(timing.mutex);
-        timed = timing.enabled;
-    }
+    timed = timing.enabled.load();
+    note_launches(1 + 3ull * (params.maximum_depth + 1) + (init.capture ? 1 : 0));
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
     unsigned long long before[2] = {0, 0};
     if (timed) {
@@ -907,6 +905,7 @@ void render_tile(const Scene& scene, const IntegratorParams& params, const mr_re
             init.seed   = render.seed;
             init.count  = static_cast<uint32_t>(a * init.ns);
             Engine::run_wave(scene, params, init, ws, stream);
+            note_launches(1);
             resolve_kernel<<<static_cast<unsigned>((a + 255) / 256), 256, 0, stream>>>(
                 ws.state.radiance, init.x0, init.y0, w, hh, init.ns, init.width, accumulator,
                 ws.queues.error);
@@ -927,6 +926,7 @@ void render_frame(const Scene& scene, const IntegratorParams& params, const mr_r
     render_tile(scene, params, render, 0, 0, static_cast<uint32_t>(render.width),
                 static_cast<uint32_t>(render.height), 0, render.samples_per_pixel, ws->accumulator,
                 *ws, stream);
+    note_launches(1);
     finalize_kernel<<<static_cast<unsigned>((pixels + 255) / 256), 256, 0, stream>>>(
         ws->accumulator, pixels, render.samples_per_pixel, device_rgb, ws->queues.error);
     MR_CUDA(cudaGetLastError());

@@ -1,6 +1,7 @@
 // wavefront.cuh — path state, queues and the wavefront driver interface.
 #pragma once
 
+#include <atomic>
 #include <mutex>
 #include <vector>
 
@@ -130,12 +131,21 @@ void                       release_workspace(std::shared_ptr<Workspace> ws);
 // Kernel timing for roofline figures (nearest-hit traversal launches).
 struct KernelTiming {
     std::mutex         mutex;
-    bool               enabled  = false;
+    std::atomic<bool>  enabled{false};
+    std::atomic<uint64_t> all_launches{0};
     uint64_t           launches = 0;
     double             seconds  = 0;
     mr_trace_statistics counted{};
 };
 KernelTiming& kernel_timing();
+
+// Counts kernel launches for mr_kernel_timing while timing is enabled.
+inline void note_launches(uint64_t n) {
+    KernelTiming& t = kernel_timing();
+    if (t.enabled.load(std::memory_order_relaxed)) {
+        t.all_launches.fetch_add(n, std::memory_order_relaxed);
+    }
+}
 
 // Frame render into a device image (width*height*3 floats) — used by mr_render(_device) and the
 // session. Statistics (optional) are read back after the frame.
