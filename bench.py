@@ -333,7 +333,7 @@ def run_ours(args):
                    BYTES_PER_TRIANGLE_TEST * counted.triangle_tests)
     achieved = algorithmic / ksec.value / 1e9 if ksec.value > 0 else 0.0
     traffic = None
-    tfile = os.path.join(ROOT, "profiles", "extend_kernel_traffic.json")
+    tfile = os.path.join(ROOT, "profiles", "extend_kernel_traffic.txt")
     if os.path.exists(tfile):
         with open(tfile) as f:
             traffic = json.load(f).get("dram_bytes_per_launch")
