@@ -350,6 +350,25 @@ mr_status mr_capture_shadow_rays(const mr_scene* scene, const mr_integrator_sett
                                  const uint64_t* samples, size_t count, mr_ray* shadow_rays,
                                  uint8_t* has_shadow, uint8_t* occluded);
 
+/* Largest batch mr_trace_paths_static accepts. */
+#define MR_STATIC_MAX_PATHS 16384u
+
+/* PathTracer::trace for up to MR_STATIC_MAX_PATHS paths without allocating any memory, for
+ * callers that cannot allocate device memory while they render (for example a server that
+ * reserves its whole HBM budget in its own pool at start-up, or a loop that must not pay the
+ * device synchronisation an allocation can cause). No counterpart in the reference: it is the
+ * allocation-free form of mr_trace_paths (same per-path results). `device_rays`, `device_keys`
+ * (seed, pixel, sample per path) and `device_radiance` (3 floats per path) are device memory;
+ * `stream` is a cudaStream_t (null = legacy default stream); the call returns after the work
+ * has finished. The working memory is one fixed array of about 4.2 MB inside the library, held
+ * on every GPU that loads it until the process exits; the first call on a device looks up its
+ * address and should come before any stream capture. Calls share that array: it is cleared at
+ * the start of each call, and calls whose GPU work overlaps race. Larger batches are rejected
+ * with MR_INVALID_ARGUMENT. */
+mr_status mr_trace_paths_static(const mr_scene* scene, const mr_integrator_settings* integrator,
+                                const mr_ray* device_rays, const uint64_t* device_keys,
+                                size_t count, float* device_radiance, void* stream);
+
 /* ---- render ----------------------------------------------------------------------------- */
 
 /* PathTracer::render (src/render/path_tracer.cpp:521-538): writes width*height*3 floats of

@@ -184,6 +184,7 @@ SIGNATURES = {
     "mr_capture_shadow_rays": (C.c_int, [VP, P(IntegratorSettings), P(RenderSettings),
                                          P(C.c_uint32), P(C.c_uint64), C.c_size_t, P(Ray),
                                          P(C.c_uint8), P(C.c_uint8)]),
+    "mr_trace_paths_static": (C.c_int, [VP, P(IntegratorSettings), VP, VP, C.c_size_t, VP, VP]),
     "mr_render": (C.c_int, [VP, P(IntegratorSettings), P(RenderSettings), P(C.c_float),
                             P(PathStatistics)]),
     "mr_render_device": (C.c_int, [VP, P(IntegratorSettings), P(RenderSettings), VP, VP,

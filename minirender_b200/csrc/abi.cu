@@ -448,6 +448,10 @@ void session_run(mr_session* s, const Scene* scene, IntegratorParams params, mr_
 }
 
 }  // namespace
+
+// Lets the other C-ABI translation units report through mr_last_error.
+void set_last_error(const std::string& message) { last_error = message; }
+
 }  // namespace mr
 
 using namespace mr;
