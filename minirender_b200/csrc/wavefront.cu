@@ -151,8 +151,9 @@ __global__ void init_rays_kernel(KernelArgs a, WaveInit w) {
 
 // ---- extend ----
 
+// 8 resident blocks per SM (<= 64 registers): the traversal is latency bound, warps hide it.
 template <bool MEDIA>
-__global__ void __launch_bounds__(128) extend_kernel(KernelArgs a) {
+__global__ void __launch_bounds__(128, 8) extend_kernel(KernelArgs a) {
     BounceCounters* ctr   = a.q.counters + a.bounce;
     const uint32_t  count = ctr->ext;
     const uint32_t* in    = a.q.ext[a.bounce & 1];
@@ -465,7 +466,7 @@ __global__ void __launch_bounds__(128) shade_kernel(KernelArgs a) {
 // ---- shadow ----
 
 template <bool MEDIA>
-__global__ void __launch_bounds__(128) shadow_kernel(KernelArgs a) {
+__global__ void __launch_bounds__(128, 8) shadow_kernel(KernelArgs a) {
     BounceCounters* ctr   = a.q.counters + a.bounce;
     const uint32_t  count = ctr->shadow;
     TraceCounters   tc{0, 0};
