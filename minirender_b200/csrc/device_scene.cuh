@@ -1,15 +1,14 @@
 // device_scene.cuh — the scene as it lives in HBM.
 //
 // Traversal data and shading data are separate streams, each an array of 16-byte records:
-//  - nodes:  4 float4 per interior node. Both children's boxes sit in the parent, so one node
-//            fetch (64 B, 4 x LDG.128) serves the two slab tests the reference performs per
-//            interior node (src/render/bvh.cpp:393-406).
-//              [0] = (lo.x, hi.x, lo.y, hi.y) of the left child
-//              [1] = (lo.x, hi.x, lo.y, hi.y) of the right child
-//              [2] = (lo.z, hi.z) left, (lo.z, hi.z) right
-//              [3] = (left ref, right ref, left count, right count) as int bits
-//            A child ref >= 0 is an interior node index; a ref < 0 is a leaf whose triangles
-//            occupy slots [~ref, ~ref + count) of the triangle stream.
+//  - nodes:  8 float4 (128 B, one cache line) per 4-wide node collapsed from the binary SAH
+//            tree. One fetch serves up to four slab tests, so a ray needs about half as many
+//            dependent node fetches as on the binary tree.
+//              [0..5] = lo.x, hi.x, lo.y, hi.y, lo.z, hi.z of children 0..3 (x4 vectors;
+//                       unused children hold an empty box)
+//              [6]    = child refs (int bits): >= 0 wide node index; < 0 leaf whose triangles
+//                       occupy slots ~ref .. the slot flagged kTriLeafEnd
+//              [7].x  = number of children (int bits)
 //  - tris:   3 float4 per triangle slot, in leaf order (no index indirection during traversal):
 //              [0] = v0.xyz, flat primitive id (uint bits)
 //              [1] = v1.xyz, flags (uint bits: kTriSingleSided | kTriMirrored | kind << 8)

@@ -114,35 +114,103 @@ __global__ void flatten_kernel(const float* positions, const mr_mesh_corner* cor
     centroid[p] = f4(third, 0.0f);
 }
 
-// Interior-node flags for the rank scan.
-__global__ void interior_flag_kernel(const mr_bvh_node* nodes, uint32_t count, uint32_t* flags) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < count) {
-        flags[i] = nodes[i].count == 0 ? 1u : 0u;
-    }
+// Collapse of the binary tree (reference layout) into 4-wide traversal nodes, one level of wide
+// nodes per launch pair. A wide node starts from a binary interior node's two children and
+// repeatedly opens the interior child with the largest surface area until it has four children
+// or only leaves remain.
+__device__ __forceinline__ float node_area(const mr_bvh_node& n) {
+    const float ex = n.maximum[0] - n.minimum[0], ey = n.maximum[1] - n.minimum[1],
+                ez = n.maximum[2] - n.minimum[2];
+    return ex * ey + ey * ez + ez * ex;
 }
 
-__device__ __forceinline__ int child_ref(const mr_bvh_node* nodes, const uint32_t* rank,
-                                         uint32_t child) {
-    const mr_bvh_node& c = nodes[child];
-    return c.count == 0 ? static_cast<int>(rank[child]) : ~static_cast<int>(c.first);
-}
-
-// Reference-layout nodes -> traversal nodes (children's boxes stored in the parent).
-__global__ void convert_nodes_kernel(const mr_bvh_node* nodes, const uint32_t* rank,
-                                     uint32_t count, float4* out) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= count || nodes[i].count != 0) {
+__global__ void collapse_count_kernel(const mr_bvh_node* nodes, const uint32_t* roots, uint32_t count,
+                                      int4* children, uint32_t* interior_counts) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count) {
         return;
     }
-    const mr_bvh_node& l = nodes[nodes[i].first];
-    const mr_bvh_node& r = nodes[nodes[i].right];
-    float4*            o = out + 4 * static_cast<size_t>(rank[i]);
-    o[0] = make_float4(l.minimum[0], l.maximum[0], l.minimum[1], l.maximum[1]);
-    o[1] = make_float4(r.minimum[0], r.maximum[0], r.minimum[1], r.maximum[1]);
-    o[2] = make_float4(l.minimum[2], l.maximum[2], r.minimum[2], r.maximum[2]);
-    o[3] = make_float4(__int_as_float(child_ref(nodes, rank, nodes[i].first)),
-                       __int_as_float(child_ref(nodes, rank, nodes[i].right)), 0.0f, 0.0f);
+    const mr_bvh_node& root = nodes[roots[k]];
+    int c[4] = {static_cast<int>(root.first), static_cast<int>(root.right), -1, -1};
+    int n    = 2;
+    while (n < 4) {
+        int   best = -1;
+        float area = -1.0f;
+        for (int i = 0; i < n; ++i) {
+            const mr_bvh_node& child = nodes[c[i]];
+            if (child.count == 0 && node_area(child) > area) {
+                area = node_area(child);
+                best = i;
+            }
+        }
+        if (best < 0) {
+            break;
+        }
+        const mr_bvh_node& open = nodes[c[best]];
+        c[best]  = static_cast<int>(open.first);
+        c[n++]   = static_cast<int>(open.right);
+    }
+    uint32_t interior = 0;
+    for (int i = 0; i < n; ++i) {
+        interior += nodes[c[i]].count == 0 ? 1u : 0u;
+    }
+    children[k]        = make_int4(c[0], c[1], c[2], c[3]);
+    interior_counts[k] = interior;
+}
+
+// Writes wide node `base + k`: children's boxes as six x4 vectors, refs, child count.
+__global__ void collapse_write_kernel(const mr_bvh_node* nodes, const int4* children, uint32_t count,
+                                      const uint32_t* offsets, uint32_t base, uint32_t next_base,
+                                      float4* wide, uint32_t* next_roots) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count) {
+        return;
+    }
+    const int4 c4   = children[k];
+    const int  c[4] = {c4.x, c4.y, c4.z, c4.w};
+    float      lo[3][4], hi[3][4];
+    int        ref[4];
+    int        valid = 0;
+    uint32_t   rank  = 0;
+    for (int i = 0; i < 4; ++i) {
+        if (c[i] < 0) {
+            for (int a = 0; a < 3; ++a) {
+                lo[a][i] = INFINITY;  // empty box: every slab test misses
+                hi[a][i] = -INFINITY;
+            }
+            ref[i] = 0;
+            continue;
+        }
+        const mr_bvh_node& n = nodes[c[i]];
+        for (int a = 0; a < 3; ++a) {
+            lo[a][i] = n.minimum[a];
+            hi[a][i] = n.maximum[a];
+        }
+        if (n.count == 0) {
+            const uint32_t slot = offsets[k] + rank++;
+            next_roots[slot]    = static_cast<uint32_t>(c[i]);
+            ref[i]              = static_cast<int>(next_base + slot);
+        } else {
+            ref[i] = ~static_cast<int>(n.first);
+        }
+        ++valid;
+    }
+    float4* o = wide + 8 * static_cast<size_t>(base + k);
+    for (int a = 0; a < 3; ++a) {
+        o[2 * a]     = make_float4(lo[a][0], lo[a][1], lo[a][2], lo[a][3]);
+        o[2 * a + 1] = make_float4(hi[a][0], hi[a][1], hi[a][2], hi[a][3]);
+    }
+    o[6] = make_float4(__int_as_float(ref[0]), __int_as_float(ref[1]), __int_as_float(ref[2]),
+                       __int_as_float(ref[3]));
+    o[7] = make_float4(__int_as_float(valid), 0.0f, 0.0f, 0.0f);
+}
+
+__global__ void interior_count_kernel(const mr_bvh_node* nodes, uint32_t count, uint32_t* total) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const unsigned m = __ballot_sync(0xffffffffu, i < count && nodes[i].count == 0);
+    if ((threadIdx.x & 31) == 0 && m) {
+        atomicAdd(total, static_cast<uint32_t>(__popc(m)));
+    }
 }
 
 // Triangle stream in leaf order; marks the last slot of every leaf.
@@ -477,22 +545,43 @@ std::unique_ptr<Scene> create_scene(const mr_scene_desc& desc, const mr_bvh_desc
     hi.release();
     centroid.release();
 
-    // ---- traversal layout ----
-    uint32_t interior = 0;
+    // ---- traversal layout: 4-wide nodes collapsed from the binary tree ----
+    uint32_t wide_count = 0;
     if (prims) {
-        DeviceBuffer<uint32_t> flags, rank, scratch, total_interior;
-        flags.allocate(node_count);
-        rank.allocate(node_count);
-        scratch.allocate(scan_scratch_size(node_count));
-        total_interior.allocate(1);
-        interior_flag_kernel<<<(node_count + 255) / 256, 256, 0, stream>>>(ref_nodes.ptr, node_count, flags.ptr);
-        exclusive_scan(flags.ptr, rank.ptr, node_count, scratch.ptr, total_interior.ptr, stream);
-        MR_CUDA(cudaMemcpyAsync(&interior, total_interior.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+        DeviceBuffer<uint32_t> total;
+        total.allocate(1);
+        MR_CUDA(cudaMemsetAsync(total.ptr, 0, sizeof(uint32_t), stream));
+        interior_count_kernel<<<(node_count + 255) / 256, 256, 0, stream>>>(ref_nodes.ptr, node_count, total.ptr);
+        uint32_t interior = 0;
+        MR_CUDA(cudaMemcpyAsync(&interior, total.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
         MR_CUDA(cudaStreamSynchronize(stream));
-        scene->nodes.allocate(std::max<uint32_t>(1, interior) * 4ull);
+        scene->nodes.allocate(std::max<uint32_t>(1, interior) * 8ull);
         if (interior) {
-            convert_nodes_kernel<<<(node_count + 255) / 256, 256, 0, stream>>>(ref_nodes.ptr, rank.ptr,
-                                                                                 node_count, scene->nodes.ptr);
+            DeviceBuffer<uint32_t> roots[2], counts, offsets, scratch;
+            DeviceBuffer<int4>     children;
+            roots[0].allocate(interior);
+            roots[1].allocate(interior);
+            counts.allocate(interior);
+            offsets.allocate(interior);
+            children.allocate(interior);
+            scratch.allocate(scan_scratch_size(interior));
+            MR_CUDA(cudaMemsetAsync(roots[0].ptr, 0, sizeof(uint32_t), stream));  // the root
+            uint32_t level = 1, base = 0, cur = 0;
+            while (level > 0) {
+                collapse_count_kernel<<<(level + 127) / 128, 128, 0, stream>>>(ref_nodes.ptr, roots[cur].ptr,
+                                                                               level, children.ptr, counts.ptr);
+                exclusive_scan(counts.ptr, offsets.ptr, level, scratch.ptr, total.ptr, stream);
+                collapse_write_kernel<<<(level + 127) / 128, 128, 0, stream>>>(
+                    ref_nodes.ptr, children.ptr, level, offsets.ptr, base, base + level, scene->nodes.ptr,
+                    roots[cur ^ 1].ptr);
+                uint32_t next = 0;
+                MR_CUDA(cudaMemcpyAsync(&next, total.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+                MR_CUDA(cudaStreamSynchronize(stream));
+                base += level;
+                level = next;
+                cur ^= 1;
+            }
+            wide_count = base;
         }
         scene->tris.allocate(3ull * prims);
         gather_triangles_kernel<<<(prims + 255) / 256, 256, 0, stream>>>(world.ptr, ref_order.ptr, prims,
@@ -511,7 +600,7 @@ std::unique_ptr<Scene> create_scene(const mr_scene_desc& desc, const mr_bvh_desc
             scene->d.root_hi[a] = root.maximum[a];
         }
     }
-    scene->d.node_count = interior;
+    scene->d.node_count = wide_count;
     scene->ref_nodes    = std::move(ref_nodes);
     scene->ref_order    = std::move(ref_order);
 

@@ -15,7 +15,7 @@
 
 namespace mr {
 
-constexpr int      kStackSize  = 64;  // trees are at most 48 levels deep (bvh.cpp:126)
+constexpr int      kStackSize  = 145;  // a wide node pushes <= 3 entries; <= 48 levels (bvh.cpp:126)
 constexpr uint32_t kMaxVisits  = 1u << 16;  // node visits per ray before the query gives up
 
 struct RayQuery {
@@ -72,6 +72,23 @@ __device__ __forceinline__ float slab_enter(const RayQuery& q, float4 xy, float 
     const float enter = fmaxf(fmaxf(tmin, nx), fmaxf(ny, nz));
     const float leave = fminf(fminf(tmax, fx), fminf(fy, fz));
     return enter <= leave ? enter : __int_as_float(0x7fffffff);
+}
+
+// Slab test of one child of a wide node (six scalar bounds); NaN when missed.
+__device__ __forceinline__ float slab_enter6(const RayQuery& q, float lx, float hx, float ly, float hy,
+                                             float lz, float hz, float tmin, float tmax) {
+    return slab_enter(q, make_float4(lx, hx, ly, hy), lz, hz, tmin, tmax);
+}
+
+__device__ __forceinline__ void order2(float& ta, int& ra, float& tb, int& rb) {
+    if (tb < ta) {
+        const float t = ta;
+        ta            = tb;
+        tb            = t;
+        const int r   = ra;
+        ra            = rb;
+        rb            = r;
+    }
 }
 
 __device__ __forceinline__ float permuted(f3 v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
@@ -175,31 +192,46 @@ __device__ __forceinline__ TraceResult trace(const DeviceScene& s, const RayQuer
             return result;
         }
         if (node >= 0) {
-            const float4* n  = s.nodes + 4 * static_cast<size_t>(node);
-            const float4  lxy = __ldg(n + 0);
-            const float4  rxy = __ldg(n + 1);
-            const float4  z   = __ldg(n + 2);
-            const int4    lk  = __ldg(reinterpret_cast<const int4*>(n + 3));
-            counters.bounds += 2;
-            const float tl = slab_enter(q, lxy, z.x, z.y, tmin, result.t);
-            const float tr = slab_enter(q, rxy, z.z, z.w, tmin, result.t);
-            const bool  hl = tl <= result.t;
-            const bool  hr = tr <= result.t;
-            if (hl && hr) {
-                const bool left_nearer = tl <= tr;
-                if (sp == kStackSize) {
+            // Wide node: four slab tests, children visited near to far (the reference's
+            // near-first order generalised; results do not depend on the order).
+            const float4* n   = s.nodes + 8 * static_cast<size_t>(node);
+            const float4  lox = __ldg(n + 0), hix = __ldg(n + 1);
+            const float4  loy = __ldg(n + 2), hiy = __ldg(n + 3);
+            const float4  loz = __ldg(n + 4), hiz = __ldg(n + 5);
+            const int4    ref = __ldg(reinterpret_cast<const int4*>(n + 6));
+            counters.bounds += static_cast<uint32_t>(__ldg(reinterpret_cast<const int*>(n + 7)));
+            const float inf = __int_as_float(0x7f800000);
+            float t0 = slab_enter6(q, lox.x, hix.x, loy.x, hiy.x, loz.x, hiz.x, tmin, result.t);
+            float t1 = slab_enter6(q, lox.y, hix.y, loy.y, hiy.y, loz.y, hiz.y, tmin, result.t);
+            float t2 = slab_enter6(q, lox.z, hix.z, loy.z, hiy.z, loz.z, hiz.z, tmin, result.t);
+            float t3 = slab_enter6(q, lox.w, hix.w, loy.w, hiy.w, loz.w, hiz.w, tmin, result.t);
+            t0 = t0 <= result.t ? t0 : inf;
+            t1 = t1 <= result.t ? t1 : inf;
+            t2 = t2 <= result.t ? t2 : inf;
+            t3 = t3 <= result.t ? t3 : inf;
+            int r0 = ref.x, r1 = ref.y, r2 = ref.z, r3 = ref.w;
+            order2(t0, r0, t1, r1);
+            order2(t2, r2, t3, r3);
+            order2(t0, r0, t2, r2);
+            order2(t1, r1, t3, r3);
+            order2(t1, r1, t2, r2);
+            if (t0 != inf) {
+                const int pushes = (t1 != inf) + (t2 != inf) + (t3 != inf);
+                if (sp + pushes > kStackSize) {
                     error |= kErrorStack;
                     return result;
                 }
-                stack[sp++] = left_nearer ? make_int2(lk.y, __float_as_int(tr))
-                                          : make_int2(lk.x, __float_as_int(tl));
-                node      = left_nearer ? lk.x : lk.y;
-                node_tmin = left_nearer ? tl : tr;
-                continue;
-            }
-            if (hl || hr) {
-                node      = hl ? lk.x : lk.y;
-                node_tmin = hl ? tl : tr;
+                if (t3 != inf) {
+                    stack[sp++] = make_int2(r3, __float_as_int(t3));
+                }
+                if (t2 != inf) {
+                    stack[sp++] = make_int2(r2, __float_as_int(t2));
+                }
+                if (t1 != inf) {
+                    stack[sp++] = make_int2(r1, __float_as_int(t1));
+                }
+                node      = r0;
+                node_tmin = t0;
                 continue;
             }
         } else {
