@@ -149,15 +149,87 @@ __global__ void init_rays_kernel(KernelArgs a, WaveInit w) {
     }
 }
 
-// ---- extend ----
+// ---- trace: this bounce's nearest-hit queue + the previous bounce's shadow queue ----
 
-// 8 resident blocks per SM (<= 64 registers): the traversal is latency bound, warps hide it.
+// Nearest hit of one extension ray, its material bin (or kNone) and, with media, the
+// free-flight sample over the hit interval.
 template <bool MEDIA>
-__global__ void __launch_bounds__(128, 8) extend_kernel(KernelArgs a) {
-    BounceCounters* ctr   = a.q.counters + a.bounce;
-    const uint32_t  count = ctr->ext;
-    const uint32_t* in    = a.q.ext[a.bounce & 1];
-    TraceCounters   tc{0, 0};
+__device__ __forceinline__ uint32_t extend_item(const KernelArgs& a, uint32_t path, TraceCounters& tc,
+                                                unsigned& error) {
+    const float4 o4 = a.st.ray_o[path];
+    const float4 d4 = a.st.ray_d[path];
+    RayQuery     q;
+    q.init(xyz(o4), xyz(d4));
+    const TraceResult r    = trace<false>(a.scene, q, o4.w, d4.w, tc, error);
+    uint32_t          kind = 0;
+    if (r.slot != kNone) {
+        a.st.hit[path] = make_float4(r.t, __fdiv_rn(r.a, r.det), __fdiv_rn(r.b, r.det),
+                                     __fdiv_rn(r.c, r.det));
+        kind = (__float_as_uint(__ldg(a.scene.tris + 3 * static_cast<size_t>(r.slot) + 1).w) >> 8) & 0xffu;
+    }
+    a.st.hit_slot[path] = r.slot;
+    uint32_t key        = r.slot == kNone ? kBinMiss : kBinDiffuse + kind;
+    if (MEDIA && a.scene.medium_count > 0) {
+        // MediumField::sample over [minimum, hit ? distance : maximum]
+        // (src/render/path_tracer.cpp:303-310).
+        Pcg32  rng   = load_rng(a.st, path);
+        float4 beta4 = a.st.beta[path];
+        bool   scattered;
+        float  scatter_t = 0, g = 0;
+        const f3 w = field_sample(a.scene, xyz(o4), xyz(d4), o4.w, r.slot != kNone ? r.t : d4.w, rng,
+                                  scattered, scatter_t, g, error);
+        f3 beta = xyz(beta4) * w;
+        store_rng(a.st, path, rng);
+        a.st.beta[path] = f4(beta, beta4.w);
+        if (!finite3(beta) || beta.x < 0 || beta.y < 0 || beta.z < 0) {
+            error |= kErrorRadiance;
+            key = kNone;
+        } else if (max3(beta) == 0) {
+            key = kNone;
+        } else if (scattered) {
+            a.st.hit[path] = make_float4(scatter_t, g, 0, 0);
+            key            = kBinMedium;
+        }
+    }
+    return key;
+}
+
+// Any hit of one shadow segment; adds the contribution (times the media transmittance) when
+// the segment is clear.
+template <bool MEDIA>
+__device__ __forceinline__ void shadow_item(const KernelArgs& a, uint32_t path, TraceCounters& tc,
+                                            unsigned& error) {
+    const float4 o4 = a.st.shadow_o[path];
+    const float4 d4 = a.st.shadow_d[path];
+    RayQuery     q;
+    q.init(xyz(o4), xyz(d4));
+    const TraceResult r = trace<true>(a.scene, q, 0.0f, o4.w, tc, error);
+    if (a.occluded_out) {
+        a.occluded_out[path] = r.slot != kNone ? 1 : 0;
+    }
+    if (r.slot == kNone) {
+        f3 c = xyz(a.st.shadow_c[path]);
+        if (MEDIA && a.scene.medium_count > 0) {
+            c = c * field_transmittance(a.scene, xyz(o4), xyz(d4), 0.0f, o4.w);
+        }
+        const float4 L      = a.st.radiance[path];
+        a.st.radiance[path] = make_float4(L.x + c.x, L.y + c.y, L.z + c.z, 0);
+    }
+}
+
+// One persistent launch per bounce traverses both queues: the bounce's extension rays first,
+// then the shadow segments the previous bounce's shading queued (their contributions land
+// before this bounce's shading adds emission, the reference's accumulation order). Warps fetch
+// 32 consecutive items, so only the warp at the boundary mixes the two kinds. 8 resident blocks
+// per SM (<= 64 registers): the traversal is latency bound and more warps hide it.
+template <bool MEDIA>
+__global__ void __launch_bounds__(128, 8) trace_kernel(KernelArgs a) {
+    BounceCounters* ctr      = a.q.counters + a.bounce;
+    const uint32_t  n_ext    = ctr->ext;
+    const uint32_t  n_shadow = a.bounce > 0 ? a.q.counters[a.bounce - 1].shadow : 0;
+    const uint32_t  total    = n_ext + n_shadow;
+    const uint32_t* in       = a.q.ext[a.bounce & 1];
+    TraceCounters   tc_ext{0, 0}, tc_shadow{0, 0};
     unsigned        error = 0;
     const int       lane  = lane_id();
     while (true) {
@@ -166,55 +238,26 @@ __global__ void __launch_bounds__(128, 8) extend_kernel(KernelArgs a) {
             base = atomicAdd(&ctr->work_extend, 32u);
         }
         base = __shfl_sync(0xffffffffu, base, 0);
-        if (base >= count) {
+        if (base >= total) {
             break;
         }
-        const uint32_t i   = base + lane;
-        uint32_t       key = kNone;
+        const uint32_t i    = base + lane;
+        uint32_t       key  = kNone;
         uint32_t       path = 0;
-        if (i < count) {
-            path            = in[i];
-            const float4 o4 = a.st.ray_o[path];
-            const float4 d4 = a.st.ray_d[path];
-            RayQuery     q;
-            q.init(xyz(o4), xyz(d4));
-            const TraceResult r = trace<false>(a.scene, q, o4.w, d4.w, tc, error);
-            uint32_t          kind = 0;
-            if (r.slot != kNone) {
-                a.st.hit[path] = make_float4(r.t, __fdiv_rn(r.a, r.det), __fdiv_rn(r.b, r.det),
-                                             __fdiv_rn(r.c, r.det));
-                kind = (__float_as_uint(__ldg(a.scene.tris + 3 * static_cast<size_t>(r.slot) + 1).w) >> 8) & 0xffu;
-            }
-            a.st.hit_slot[path] = r.slot;
-            key = r.slot == kNone ? kBinMiss : kBinDiffuse + kind;
-            if (MEDIA && a.scene.medium_count > 0) {
-                // MediumField::sample over [minimum, hit ? distance : maximum]
-                // (src/render/path_tracer.cpp:303-310).
-                Pcg32  rng   = load_rng(a.st, path);
-                float4 beta4 = a.st.beta[path];
-                bool   scattered;
-                float  scatter_t = 0, g = 0;
-                const f3 w = field_sample(a.scene, xyz(o4), xyz(d4), o4.w,
-                                          r.slot != kNone ? r.t : d4.w, rng, scattered, scatter_t, g,
-                                          error);
-                f3 beta = xyz(beta4) * w;
-                store_rng(a.st, path, rng);
-                a.st.beta[path] = f4(beta, beta4.w);
-                if (!finite3(beta) || beta.x < 0 || beta.y < 0 || beta.z < 0) {
-                    error |= kErrorRadiance;
-                    key = kNone;
-                } else if (max3(beta) == 0) {
-                    key = kNone;
-                } else if (scattered) {
-                    a.st.hit[path] = make_float4(scatter_t, g, 0, 0);
-                    key            = kBinMedium;
-                }
-            }
+        if (i < n_ext) {
+            path = in[i];
+            key  = extend_item<MEDIA>(a, path, tc_ext, error);
+        } else if (i < total) {
+            shadow_item<MEDIA>(a, a.q.shadow[i - n_ext], tc_shadow, error);
         }
-        warp_append(key, path, ctr->bins, a.q.bins, a.capacity);
+        if (base < n_ext) {
+            warp_append(key, path, ctr->bins, a.q.bins, a.capacity);
+        }
     }
-    warp_add_stat(a.q.stats + kStatExtendBounds, tc.bounds);
-    warp_add_stat(a.q.stats + kStatExtendTriangles, tc.triangles);
+    warp_add_stat(a.q.stats + kStatExtendBounds, tc_ext.bounds);
+    warp_add_stat(a.q.stats + kStatExtendTriangles, tc_ext.triangles);
+    warp_add_stat(a.q.stats + kStatShadowBounds, tc_shadow.bounds);
+    warp_add_stat(a.q.stats + kStatShadowTriangles, tc_shadow.triangles);
     if (error) {
         atomicOr(a.q.error, error);
     }
@@ -463,52 +506,6 @@ __global__ void __launch_bounds__(128) shade_kernel(KernelArgs a) {
     }
 }
 
-// ---- shadow ----
-
-template <bool MEDIA>
-__global__ void __launch_bounds__(128, 8) shadow_kernel(KernelArgs a) {
-    BounceCounters* ctr   = a.q.counters + a.bounce;
-    const uint32_t  count = ctr->shadow;
-    TraceCounters   tc{0, 0};
-    unsigned        error = 0;
-    const int       lane  = lane_id();
-    while (true) {
-        uint32_t base = 0;
-        if (lane == 0) {
-            base = atomicAdd(&ctr->work_shadow, 32u);
-        }
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (base >= count) {
-            break;
-        }
-        const uint32_t i = base + lane;
-        if (i < count) {
-            const uint32_t path = a.q.shadow[i];
-            const float4   o4   = a.st.shadow_o[path];
-            const float4   d4   = a.st.shadow_d[path];
-            RayQuery       q;
-            q.init(xyz(o4), xyz(d4));
-            const TraceResult r = trace<true>(a.scene, q, 0.0f, o4.w, tc, error);
-            if (a.occluded_out) {
-                a.occluded_out[path] = r.slot != kNone ? 1 : 0;
-            }
-            if (r.slot == kNone) {
-                f3 c = xyz(a.st.shadow_c[path]);
-                if (MEDIA && a.scene.medium_count > 0) {
-                    c = c * field_transmittance(a.scene, xyz(o4), xyz(d4), 0.0f, o4.w);
-                }
-                float4 L = a.st.radiance[path];
-                a.st.radiance[path] = make_float4(L.x + c.x, L.y + c.y, L.z + c.z, 0);
-            }
-        }
-    }
-    warp_add_stat(a.q.stats + kStatShadowBounds, tc.bounds);
-    warp_add_stat(a.q.stats + kStatShadowTriangles, tc.triangles);
-    if (error) {
-        atomicOr(a.q.error, error);
-    }
-}
-
 // ---- pixel accumulation ----
 
 __device__ __forceinline__ void neumaier(float& sum, float& comp, float v) {
@@ -590,9 +587,8 @@ __global__ void copy_radiance_kernel(const float4* radiance, uint32_t count, flo
 // ---- launch helpers ----
 
 struct LaunchShape {
-    int extend_blocks[2]  = {0, 0};
-    int shade_blocks      = 0;
-    int shadow_blocks[2]  = {0, 0};
+    int trace_blocks[2] = {0, 0};
+    int shade_blocks    = 0;
 };
 
 LaunchShape& launch_shape() {
@@ -604,16 +600,12 @@ LaunchShape& launch_shape() {
         int sms = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, current);
         int per = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, extend_kernel<false>, 128, 0);
-        shape.extend_blocks[0] = sms * std::max(1, per);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, extend_kernel<true>, 128, 0);
-        shape.extend_blocks[1] = sms * std::max(1, per);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, trace_kernel<false>, 128, 0);
+        shape.trace_blocks[0] = sms * std::max(1, per);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, trace_kernel<true>, 128, 0);
+        shape.trace_blocks[1] = sms * std::max(1, per);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, shade_kernel, 128, 0);
         shape.shade_blocks = sms * std::max(1, per);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, shadow_kernel<false>, 128, 0);
-        shape.shadow_blocks[0] = sms * std::max(1, per);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, shadow_kernel<true>, 128, 0);
-        shape.shadow_blocks[1] = sms * std::max(1, per);
         device = current;
     }
     return shape;
@@ -818,9 +810,10 @@ void Engine::run_wave(const Scene& scene, const IntegratorParams& params, const 
     KernelTiming&      timing = kernel_timing();
     bool               timed  = false;
     timed = timing.enabled.load();
-    note_launches(1 + 3ull * (params.maximum_depth + 1) + (init.capture ? 1 : 0));
+    note_launches(1 + 2ull * (params.maximum_depth + 1) + (init.capture ? 1 : 0));
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
-    unsigned long long before[2] = {0, 0};
+    // The timed launches are the trace kernels: nearest-hit and shadow tests both count.
+    unsigned long long before[4] = {0, 0, 0, 0};
     if (timed) {
         MR_CUDA(cudaMemcpyAsync(before, ws.queues.stats + kStatExtendBounds, sizeof(before),
                                 cudaMemcpyDeviceToHost, stream));
@@ -834,31 +827,27 @@ void Engine::run_wave(const Scene& scene, const IntegratorParams& params, const 
             cudaEventCreate(&e1);
             cudaEventRecord(e0, stream);
         }
+        // The first shadow rays (queued by bounce 0's shading) are traced with bounce 1.
+        a.occluded_out = bounce == 1 && init.capture ? init.capture->occluded : nullptr;
         if (media) {
-            extend_kernel<true><<<shape.extend_blocks[1], 128, 0, stream>>>(a);
+            trace_kernel<true><<<shape.trace_blocks[1], 128, 0, stream>>>(a);
         } else {
-            extend_kernel<false><<<shape.extend_blocks[0], 128, 0, stream>>>(a);
+            trace_kernel<false><<<shape.trace_blocks[0], 128, 0, stream>>>(a);
         }
+        a.occluded_out = nullptr;
         if (timed) {
             cudaEventRecord(e1, stream);
             events.emplace_back(e0, e1);
         }
         shade_kernel<<<shape.shade_blocks, 128, 0, stream>>>(a);
-        a.occluded_out = bounce == 0 && init.capture ? init.capture->occluded : nullptr;
-        if (media) {
-            shadow_kernel<true><<<shape.shadow_blocks[1], 128, 0, stream>>>(a);
-        } else {
-            shadow_kernel<false><<<shape.shadow_blocks[0], 128, 0, stream>>>(a);
-        }
         if (bounce == 0 && init.capture) {
             capture_shadow_kernel<<<(init.count + 127) / 128, 128, 0, stream>>>(a, init.capture->rays,
                                                                                 init.capture->has_shadow);
         }
-        a.occluded_out = nullptr;
     }
     MR_CUDA(cudaGetLastError());
     if (timed) {
-        unsigned long long after[2] = {0, 0};
+        unsigned long long after[4] = {0, 0, 0, 0};
         MR_CUDA(cudaMemcpyAsync(after, ws.queues.stats + kStatExtendBounds, sizeof(after),
                                 cudaMemcpyDeviceToHost, stream));
         MR_CUDA(cudaStreamSynchronize(stream));
@@ -873,8 +862,8 @@ void Engine::run_wave(const Scene& scene, const IntegratorParams& params, const 
         std::lock_guard<std::mutex> lock(timing.mutex);
         timing.launches += events.size();
         timing.seconds += seconds;
-        timing.counted.bounds_tests += after[0] - before[0];
-        timing.counted.triangle_tests += after[1] - before[1];
+        timing.counted.bounds_tests += (after[0] - before[0]) + (after[2] - before[2]);
+        timing.counted.triangle_tests += (after[1] - before[1]) + (after[3] - before[3]);
     }
 }
 

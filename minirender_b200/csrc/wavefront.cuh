@@ -24,9 +24,8 @@ struct BounceCounters {
     uint32_t ext;                 // paths entering this bounce
     uint32_t bins[kBinCount];
     uint32_t shadow;
-    uint32_t work_extend;
-    uint32_t work_shadow;
-    uint32_t pad[6];
+    uint32_t work_extend;  // work fetch of the bounce's trace launch
+    uint32_t pad[7];
 };
 
 enum Stat : int {
