@@ -430,6 +430,129 @@ mr_status mr_session_preview(const mr_session* session, uint64_t maximum_dimensi
 mr_status mr_session_result(const mr_session* session, float* rgb, size_t capacity,
                             uint64_t* width, uint64_t* height);
 
+/* ---- batching and serving ------------------------------------------------------------------
+ * No reference counterpart: MiniRender renders one job per PathTracer::render or
+ * RenderSession::start call (path_tracer.hpp:82-93, render_session.hpp:91-92). These entry points
+ * render many jobs together. Their samples are packed into shared waves of GPU paths (one CUDA
+ * graph launch per wave), so small jobs fill the GPU and per-job launch and copy costs overlap.
+ * Every job's image is bitwise the image mr_render returns for the same scene and settings: the
+ * estimator, the RNG streams and the per-pixel summation order are the same. */
+
+/* Wave shape of the multi-job engine. Zero fields take the defaults (or the autotuner's pick). */
+typedef struct mr_batch_settings {
+    uint64_t wave_paths;          /* paths per wave; 0 = 1<<22 */
+    uint32_t trace_blocks_per_sm; /* resident traversal blocks (128 threads) per SM; 0 = maximum */
+    uint32_t shade_blocks_per_sm; /* resident shading blocks per SM; 0 = maximum */
+    uint32_t sort_threshold;      /* bounce queues shorter than this skip the material sort;
+                                     0 = always sort */
+    uint32_t use_graphs;          /* nonzero: each wave is one launch of a captured CUDA graph */
+    uint32_t concurrent_waves;    /* waves that run at once on separate streams (each with its own
+                                     path state), so one wave's slow last rays overlap another's
+                                     work; 0 = 2, at most 4 */
+} mr_batch_settings;
+
+/* One render of a batch: PathTracer::render's arguments plus the host image it fills. */
+typedef struct mr_batch_job {
+    const mr_scene*        scene;
+    mr_integrator_settings integrator;
+    mr_render_settings     render;
+    float*                 rgb;    /* host image, width*height*3 floats; NULL = not copied back */
+    mr_status              status; /* out: the job's own outcome */
+} mr_batch_job;
+
+typedef struct mr_batch_statistics {
+    uint64_t           waves;
+    uint64_t           segments;        /* job pieces carried by the waves */
+    uint64_t           samples;         /* camera samples rendered */
+    uint64_t           kernel_launches; /* device kernels run (inside graphs or not) */
+    uint64_t           graph_launches;
+    double             seconds;         /* wall time from the first submission to the last image */
+    double             busy_seconds;    /* device time of the waves */
+    mr_path_statistics paths;           /* summed over all jobs */
+} mr_batch_statistics;
+
+/* Renders `count` jobs together. Returns MR_OK when every job completed; otherwise the first
+ * failing job's status (each job's own status is in jobs[i].status, jobs that completed keep
+ * their images). */
+mr_status mr_render_batch(mr_batch_job* jobs, size_t count, const mr_batch_settings* settings,
+                          mr_batch_statistics* statistics);
+
+/* Autotuner: renders the calibration jobs once per candidate wave shape (paths per wave,
+ * resident blocks, sort threshold), keeps the fastest and writes it to `best` together with the
+ * samples/s it reached. Images are not copied back. */
+mr_status mr_batch_autotune(const mr_batch_job* jobs, size_t count, mr_batch_settings* best,
+                            double* samples_per_second);
+
+/* Render server: a request loop that admits jobs as they arrive, within an HBM budget for
+ * their accumulation buffers and images, keeps those buffers resident until the job ends, and
+ * packs the samples of every admitted job into shared waves (continuous batching: a job that
+ * arrives while others render joins the next wave). Scenes stay resident in their mr_scene
+ * handles, which must outlive the jobs submitted with them. */
+typedef enum mr_schedule_policy {
+    MR_SCHEDULE_SHORTEST_FIRST = 0, /* fewest remaining samples first */
+    MR_SCHEDULE_ARRIVAL        = 1  /* submission order */
+} mr_schedule_policy;
+
+typedef struct mr_server_settings {
+    uint64_t          hbm_budget_bytes; /* job buffers admitted at once; 0 = half the free memory */
+    uint32_t          max_jobs;         /* jobs admitted at once; 0 = 1024 */
+    uint32_t          policy;           /* mr_schedule_policy */
+    mr_batch_settings batch;
+} mr_server_settings;
+
+typedef enum mr_job_state {
+    MR_JOB_QUEUED    = 0, /* waiting for HBM budget */
+    MR_JOB_RUNNING   = 1,
+    MR_JOB_PAUSED    = 2,
+    MR_JOB_COMPLETED = 3, /* image in host memory */
+    MR_JOB_CANCELLED = 4,
+    MR_JOB_FAILED    = 5
+} mr_job_state;
+
+typedef struct mr_job_info {
+    uint32_t state;             /* mr_job_state */
+    uint32_t status;            /* mr_status of a failed job */
+    uint64_t total_samples;     /* width * height * samples_per_pixel */
+    uint64_t completed_samples; /* samples resolved into the accumulator */
+    double   submitted_seconds; /* server clock: seconds since mr_server_create */
+    double   admitted_seconds;  /* 0 until admitted */
+    double   finished_seconds;  /* completed, cancelled or failed; 0 before */
+    char     error[256];
+} mr_job_info;
+
+typedef struct mr_server_statistics {
+    uint64_t submitted, admitted, completed, cancelled, failed;
+    uint64_t waves, segments, samples, kernel_launches, graph_launches;
+    uint64_t resident_bytes; /* job buffers held now */
+    double   busy_seconds;   /* device time of the waves */
+    double   elapsed_seconds;
+} mr_server_statistics;
+
+typedef struct mr_server mr_server;
+
+mr_status mr_server_create(const mr_server_settings* settings, mr_server** server);
+/* Cancels the jobs that have not finished, waits for the device and frees everything. */
+mr_status mr_server_destroy(mr_server* server);
+/* Validates like mr_render; MR_OUT_OF_MEMORY when the job alone exceeds the budget. */
+mr_status mr_server_submit(mr_server* server, const mr_scene* scene, const mr_render_settings* render,
+                           const mr_integrator_settings* integrator, uint64_t* job);
+/* Pause/resume take effect at the next wave; `accepted` as RenderSession::pause/resume. */
+mr_status mr_server_pause(mr_server* server, uint64_t job, int* accepted);
+mr_status mr_server_resume(mr_server* server, uint64_t job, int* accepted);
+mr_status mr_server_cancel(mr_server* server, uint64_t job);
+/* Waits up to `milliseconds` for the job to complete, fail or be cancelled. */
+mr_status mr_server_wait(mr_server* server, uint64_t job, uint32_t milliseconds, int* finished);
+mr_status mr_server_job_info(mr_server* server, uint64_t job, mr_job_info* info);
+/* The completed image (capacity in floats); MR_OUT_OF_RANGE unless the job completed. */
+mr_status mr_server_result(mr_server* server, uint64_t job, float* rgb, size_t capacity);
+/* Progressive image of the samples issued so far (mean per pixel); `samples` receives the
+ * sample passes every pixel has. */
+mr_status mr_server_preview(mr_server* server, uint64_t job, float* rgb, size_t capacity,
+                            uint64_t* samples);
+/* Forgets a finished job and its host image. */
+mr_status mr_server_release(mr_server* server, uint64_t job);
+mr_status mr_server_get_statistics(mr_server* server, mr_server_statistics* statistics);
+
 #ifdef __cplusplus
 }
 #endif

@@ -36,6 +36,7 @@ SAMPLING_BSDF, SAMPLING_LIGHT, SAMPLING_MIS = range(3)
 SAMPLING_MODES = {"bsdf": SAMPLING_BSDF, "light": SAMPLING_LIGHT, "mis": SAMPLING_MIS}
 RENDER_STATES = ["idle", "preparing", "running", "pausing", "paused", "finalizing",
                  "cancelling", "cancelled", "completed", "failed"]
+JOB_STATES = ["queued", "running", "paused", "completed", "cancelled", "failed"]
 
 f3 = C.c_float * 3
 d3 = C.c_double * 3
@@ -164,6 +165,42 @@ class RenderPreview(C.Structure):
 # Every exported symbol of include/minirender_b200.h with its ctypes signature.
 P = C.POINTER
 VP = C.c_void_p
+class BatchSettings(C.Structure):
+    _fields_ = [("wave_paths", C.c_uint64), ("trace_blocks_per_sm", C.c_uint32),
+                ("shade_blocks_per_sm", C.c_uint32), ("sort_threshold", C.c_uint32),
+                ("use_graphs", C.c_uint32), ("concurrent_waves", C.c_uint32)]
+
+
+class BatchJob(C.Structure):
+    _fields_ = [("scene", VP), ("integrator", IntegratorSettings), ("render", RenderSettings),
+                ("rgb", P(C.c_float)), ("status", C.c_int)]
+
+
+class BatchStatistics(C.Structure):
+    _fields_ = [("waves", C.c_uint64), ("segments", C.c_uint64), ("samples", C.c_uint64),
+                ("kernel_launches", C.c_uint64), ("graph_launches", C.c_uint64),
+                ("seconds", C.c_double), ("busy_seconds", C.c_double), ("paths", PathStatistics)]
+
+
+class ServerSettings(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_uint64), ("max_jobs", C.c_uint32), ("policy", C.c_uint32),
+                ("batch", BatchSettings)]
+
+
+class JobInfo(C.Structure):
+    _fields_ = [("state", C.c_uint32), ("status", C.c_uint32), ("total_samples", C.c_uint64),
+                ("completed_samples", C.c_uint64), ("submitted_seconds", C.c_double),
+                ("admitted_seconds", C.c_double), ("finished_seconds", C.c_double),
+                ("error", C.c_char * 256)]
+
+
+class ServerStatistics(C.Structure):
+    _fields_ = [(n, C.c_uint64) for n in ("submitted", "admitted", "completed", "cancelled", "failed",
+                                          "waves", "segments", "samples", "kernel_launches",
+                                          "graph_launches", "resident_bytes")] + \
+               [("busy_seconds", C.c_double), ("elapsed_seconds", C.c_double)]
+
+
 SIGNATURES = {
     "mr_abi_version": (C.c_uint32, []),
     "mr_last_error": (C.c_size_t, [C.c_char_p, C.c_size_t]),
@@ -206,6 +243,20 @@ SIGNATURES = {
     "mr_session_progress": (C.c_int, [VP, P(RenderProgress)]),
     "mr_session_preview": (C.c_int, [VP, C.c_uint64, P(C.c_float), C.c_size_t,
                                      P(RenderPreview)]),
+    "mr_render_batch": (C.c_int, [P(BatchJob), C.c_size_t, P(BatchSettings), P(BatchStatistics)]),
+    "mr_batch_autotune": (C.c_int, [P(BatchJob), C.c_size_t, P(BatchSettings), P(C.c_double)]),
+    "mr_server_create": (C.c_int, [P(ServerSettings), P(VP)]),
+    "mr_server_destroy": (C.c_int, [VP]),
+    "mr_server_submit": (C.c_int, [VP, VP, P(RenderSettings), P(IntegratorSettings), P(C.c_uint64)]),
+    "mr_server_pause": (C.c_int, [VP, C.c_uint64, P(C.c_int)]),
+    "mr_server_resume": (C.c_int, [VP, C.c_uint64, P(C.c_int)]),
+    "mr_server_cancel": (C.c_int, [VP, C.c_uint64]),
+    "mr_server_wait": (C.c_int, [VP, C.c_uint64, C.c_uint32, P(C.c_int)]),
+    "mr_server_job_info": (C.c_int, [VP, C.c_uint64, P(JobInfo)]),
+    "mr_server_result": (C.c_int, [VP, C.c_uint64, P(C.c_float), C.c_size_t]),
+    "mr_server_preview": (C.c_int, [VP, C.c_uint64, P(C.c_float), C.c_size_t, P(C.c_uint64)]),
+    "mr_server_release": (C.c_int, [VP, C.c_uint64]),
+    "mr_server_get_statistics": (C.c_int, [VP, P(ServerStatistics)]),
     "mr_session_result": (C.c_int, [VP, P(C.c_float), C.c_size_t, P(C.c_uint64),
                                     P(C.c_uint64)]),
 }

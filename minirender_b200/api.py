@@ -19,7 +19,8 @@ from ._abi import MiniRenderError, check, load_library
 from .scene import SceneDocument, Snapshot
 
 __all__ = ["IntegratorSettings", "RenderSettings", "SessionSettings", "Scene", "PathTracer",
-           "RenderSession", "MiniRenderError", "display_image"]
+           "RenderSession", "MiniRenderError", "display_image", "BatchSettings", "BatchJob",
+           "render_batch", "autotune", "RenderServer"]
 
 
 @dataclass
@@ -335,3 +336,169 @@ class RenderSession:
         check(self.lib.mr_session_result(self.handle, _ptr(out, C.c_float), out.size, None, None),
               self.lib)
         return out
+
+
+@dataclass
+class BatchSettings:
+    """Wave shape of the multi-job engine (mr_batch_settings); zeros take the defaults."""
+
+    wave_paths: int = 0
+    trace_blocks_per_sm: int = 0
+    shade_blocks_per_sm: int = 0
+    sort_threshold: int = 0
+    use_graphs: bool = True
+    concurrent_waves: int = 0
+
+    def c(self) -> _abi.BatchSettings:
+        return _abi.BatchSettings(self.wave_paths, self.trace_blocks_per_sm,
+                                  self.shade_blocks_per_sm, self.sort_threshold,
+                                  int(self.use_graphs), self.concurrent_waves)
+
+    @staticmethod
+    def from_c(s: _abi.BatchSettings) -> "BatchSettings":
+        return BatchSettings(s.wave_paths, s.trace_blocks_per_sm, s.shade_blocks_per_sm,
+                             s.sort_threshold, bool(s.use_graphs), s.concurrent_waves)
+
+
+@dataclass
+class BatchJob:
+    """One render of a batch: a scene, its integrator and render settings."""
+
+    scene: Scene
+    render: RenderSettings
+    integrator: IntegratorSettings | None = None
+
+
+def _batch_records(jobs, images):
+    records = (_abi.BatchJob * max(1, len(jobs)))()
+    for i, job in enumerate(jobs):
+        records[i].scene = job.scene.handle
+        records[i].integrator = (job.integrator or IntegratorSettings()).c()
+        records[i].render = job.render.c()
+        records[i].rgb = _ptr(images[i], C.c_float) if images is not None else None
+    return records
+
+
+def render_batch(jobs: list[BatchJob], settings: BatchSettings | None = None):
+    """Renders many jobs together (mr_render_batch). Returns the images ((H, W, 3) float32, None
+    for a job that failed), the per-job status codes and the batch statistics."""
+    lib = load_library()
+    images = [np.zeros((j.render.height, j.render.width, 3), np.float32) for j in jobs]
+    records = _batch_records(jobs, images)
+    stats = _abi.BatchStatistics()
+    bs = (settings or BatchSettings()).c()
+    status = lib.mr_render_batch(records, len(jobs), C.byref(bs), C.byref(stats))
+    codes = [records[i].status for i in range(len(jobs))]
+    if status != _abi.MR_OK and all(c == _abi.MR_OK for c in codes):
+        check(status, lib)
+    out = [img if code == _abi.MR_OK else None for img, code in zip(images, codes)]
+    info = {k: getattr(stats, k) for k in ("waves", "segments", "samples", "kernel_launches",
+                                           "graph_launches", "seconds", "busy_seconds")}
+    info["paths"] = stats.paths.as_dict()
+    return out, codes, info
+
+
+def autotune(jobs: list[BatchJob]):
+    """Runs the calibration jobs once per candidate wave shape and returns the fastest
+    (BatchSettings, samples per second)."""
+    lib = load_library()
+    records = _batch_records(jobs, None)
+    best = _abi.BatchSettings()
+    rate = C.c_double()
+    check(lib.mr_batch_autotune(records, len(jobs), C.byref(best), C.byref(rate)), lib)
+    return BatchSettings.from_c(best), rate.value
+
+
+class RenderServer:
+    """Request loop over the GPU (mr_server_*): admits jobs by HBM budget, keeps their
+    accumulation buffers resident and renders every admitted job in shared waves."""
+
+    POLICIES = {"shortest_first": 0, "arrival": 1}
+
+    def __init__(self, hbm_budget_bytes: int = 0, max_jobs: int = 0, policy: str = "shortest_first",
+                 batch: BatchSettings | None = None):
+        self.lib = load_library()
+        s = _abi.ServerSettings(hbm_budget_bytes, max_jobs, self.POLICIES[policy],
+                                (batch or BatchSettings()).c())
+        handle = C.c_void_p()
+        check(self.lib.mr_server_create(C.byref(s), C.byref(handle)), self.lib)
+        self.handle = handle
+        self._sizes = {}
+        self._scenes = {}
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.mr_server_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def submit(self, scene: Scene, render: RenderSettings,
+               integrator: IntegratorSettings | None = None) -> int:
+        rs, it = render.c(), (integrator or IntegratorSettings()).c()
+        job = C.c_uint64()
+        check(self.lib.mr_server_submit(self.handle, scene.handle, C.byref(rs), C.byref(it),
+                                        C.byref(job)), self.lib)
+        self._sizes[job.value] = (render.height, render.width)
+        self._scenes[job.value] = scene  # scenes must outlive their jobs
+        return job.value
+
+    def pause(self, job: int) -> bool:
+        ok = C.c_int()
+        check(self.lib.mr_server_pause(self.handle, job, C.byref(ok)), self.lib)
+        return bool(ok.value)
+
+    def resume(self, job: int) -> bool:
+        ok = C.c_int()
+        check(self.lib.mr_server_resume(self.handle, job, C.byref(ok)), self.lib)
+        return bool(ok.value)
+
+    def cancel(self, job: int):
+        check(self.lib.mr_server_cancel(self.handle, job), self.lib)
+
+    def wait(self, job: int, milliseconds: int = 0xFFFFFFFF) -> bool:
+        done = C.c_int()
+        check(self.lib.mr_server_wait(self.handle, job, milliseconds, C.byref(done)), self.lib)
+        return bool(done.value)
+
+    def info(self, job: int) -> dict:
+        i = _abi.JobInfo()
+        check(self.lib.mr_server_job_info(self.handle, job, C.byref(i)), self.lib)
+        return {"state": _abi.JOB_STATES[i.state], "status": i.status,
+                "total_samples": i.total_samples, "completed_samples": i.completed_samples,
+                "submitted": i.submitted_seconds, "admitted": i.admitted_seconds,
+                "finished": i.finished_seconds, "error": i.error.decode(errors="replace")}
+
+    def result(self, job: int) -> np.ndarray:
+        h, w = self._sizes[job]
+        out = np.zeros((h, w, 3), np.float32)
+        check(self.lib.mr_server_result(self.handle, job, _ptr(out, C.c_float), out.size), self.lib)
+        return out
+
+    def preview(self, job: int):
+        h, w = self._sizes[job]
+        out = np.zeros((h, w, 3), np.float32)
+        n = C.c_uint64()
+        check(self.lib.mr_server_preview(self.handle, job, _ptr(out, C.c_float), out.size,
+                                         C.byref(n)), self.lib)
+        return out, n.value
+
+    def release(self, job: int):
+        check(self.lib.mr_server_release(self.handle, job), self.lib)
+        self._sizes.pop(job, None)
+        self._scenes.pop(job, None)
+
+    def statistics(self) -> dict:
+        s = _abi.ServerStatistics()
+        check(self.lib.mr_server_get_statistics(self.handle, C.byref(s)), self.lib)
+        return {name: getattr(s, name) for name, _ in s._fields_}

@@ -14,6 +14,7 @@
 
 #include "errors.hpp"
 #include "shading.cuh"
+#include "validation.hpp"
 #include "wavefront.cuh"
 
 struct mr_scene {
@@ -72,27 +73,6 @@ template <typename F> mr_status guarded(F&& f) {
     } catch (const std::exception& e) {
         last_error = e.what();
         return MR_RUNTIME_ERROR;
-    }
-}
-
-// IntegratorSettings::validate (src/render/path_tracer.cpp:188-197).
-IntegratorParams integrator_params(const mr_integrator_settings* s) {
-    IntegratorParams p{MR_SAMPLING_MIS, 8, 1, 3};
-    if (s) {
-        p = {s->mode, s->maximum_depth, s->russian_roulette ? 1u : 0u, s->roulette_depth};
-    }
-    require(p.mode <= MR_SAMPLING_MIS, "Sampling mode must be bsdf, light or mis");
-    require(p.maximum_depth <= 128 && p.roulette_depth <= 128,
-            "Path and roulette depths must not exceed 128");
-    return p;
-}
-
-// RenderSettings::validate (src/render/path_tracer.cpp:199-204).
-void validate_render(const mr_render_settings* r) {
-    require(r != nullptr, "Render settings are missing");
-    if (r->width == 0 || r->height == 0 || r->width > 16384 || r->height > 16384 ||
-        r->width * r->height > 64ull * 1024 * 1024 || r->samples_per_pixel == 0) {
-        fail(MR_INVALID_ARGUMENT, "Render dimensions or sample count exceed the image budget");
     }
 }
 

@@ -33,6 +33,7 @@ struct KernelArgs {
     uint32_t         capacity;
     uint32_t         bounce;
     uint8_t*         occluded_out;  // diagnostics: per-path occlusion of this bounce's shadow ray
+    const WaveDesc*  wave;          // multi-job waves: segments (scene, settings, buffers per job)
 };
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31; }
@@ -72,6 +73,42 @@ __device__ __forceinline__ void store_rng(const PathState& st, uint32_t path, co
     st.rng[path] = make_ulonglong2(r.state, r.increment);
 }
 
+// The scene and integrator settings of a path: the launch's own in a single-job wave, its
+// segment's in a multi-job wave.
+template <bool BATCH>
+__device__ __forceinline__ const WaveSegment* segment_of(const KernelArgs& a, uint32_t path) {
+    return BATCH ? a.wave->seg + a.st.segment[path] : nullptr;
+}
+
+template <bool BATCH>
+__device__ __forceinline__ const DeviceScene& scene_of(const KernelArgs& a, const WaveSegment* g) {
+    if constexpr (BATCH) {
+        return g->scene;
+    } else {
+        return a.scene;
+    }
+}
+
+template <bool BATCH>
+__device__ __forceinline__ const IntegratorParams& params_of(const KernelArgs& a, const WaveSegment* g) {
+    if constexpr (BATCH) {
+        return g->p;
+    } else {
+        return a.p;
+    }
+}
+
+// Records a path's error in the wave's word and, in a multi-job wave, in its job's word.
+template <bool BATCH>
+__device__ __forceinline__ void note_error(const WaveSegment* g, unsigned e, unsigned& error) {
+    if (e) {
+        if constexpr (BATCH) {
+            atomicOr(g->error, e);
+        }
+        error |= e;
+    }
+}
+
 __device__ __forceinline__ void init_path(const KernelArgs& a, uint32_t slot, Pcg32 rng, f3 o, f3 d,
                                           float tmin, float tmax) {
     a.st.rng[slot]      = make_ulonglong2(rng.state, rng.increment);
@@ -84,8 +121,23 @@ __device__ __forceinline__ void init_path(const KernelArgs& a, uint32_t slot, Pc
     a.q.ext[0][slot]    = slot;
 }
 
-// Camera paths of a pixel rectangle x sample range (PathTracer::sample_pixel,
+// Stream derivation, film jitter and lens sample of one camera sample (PathTracer::sample_pixel,
 // src/render/path_tracer.cpp:501-519).
+__device__ __forceinline__ CameraRay camera_sample(const CameraBasis& camera, uint32_t x, uint32_t y,
+                                                   uint64_t sample, uint32_t width, uint32_t height,
+                                                   uint64_t seed, Pcg32& rng) {
+    rng               = Pcg32::for_sample(seed, static_cast<uint64_t>(y) * width + x, sample);
+    const float fx    = rng.next_1d();
+    const float fy    = rng.next_1d();
+    const float lx    = rng.next_1d();
+    const float ly    = rng.next_1d();
+    const float u     = (static_cast<float>(x) + fx) / static_cast<float>(width);
+    const float v     = (static_cast<float>(y) + fy) / static_cast<float>(height);
+    const float aspect = static_cast<float>(width) / static_cast<float>(height);
+    return camera_ray(camera, u, v, aspect, lx, ly);
+}
+
+// Camera paths of a pixel rectangle x sample range, or of a pixel/sample list.
 __global__ void init_camera_kernel(KernelArgs a, WaveInit w) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t n = w.count;
@@ -107,15 +159,8 @@ __global__ void init_camera_kernel(KernelArgs a, WaveInit w) {
         y      = w.pixels[2 * i + 1];
         sample = w.samples[i];
     }
-    Pcg32       rng   = Pcg32::for_sample(w.seed, static_cast<uint64_t>(y) * w.width + x, sample);
-    const float fx    = rng.next_1d();
-    const float fy    = rng.next_1d();
-    const float lx    = rng.next_1d();
-    const float ly    = rng.next_1d();
-    const float u     = (static_cast<float>(x) + fx) / static_cast<float>(w.width);
-    const float v     = (static_cast<float>(y) + fy) / static_cast<float>(w.height);
-    const float aspect = static_cast<float>(w.width) / static_cast<float>(w.height);
-    const CameraRay r = camera_ray(a.scene.camera, u, v, aspect, lx, ly);
+    Pcg32           rng;
+    const CameraRay r = camera_sample(a.scene.camera, x, y, sample, w.width, w.height, w.seed, rng);
     init_path(a, i, rng, r.origin, r.direction, r.minimum, r.maximum);
     if (w.camera_rays_out) {
         w.camera_rays_out[2 * i]     = f4(r.origin, r.minimum);
@@ -127,6 +172,46 @@ __global__ void init_camera_kernel(KernelArgs a, WaveInit w) {
     if (lane_id() == 0) {
         atomicAdd(a.q.stats + kStatPaths,
                   static_cast<unsigned long long>(min(32u, n - (i & ~31u))));
+    }
+}
+
+// Segment k of a multi-job wave holding index i: the largest k < segments with first[k] <= i.
+__device__ __forceinline__ uint32_t find_segment(const uint32_t* first, uint32_t segments, uint32_t i) {
+    uint32_t lo = 0, hi = segments - 1;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1) >> 1;
+        if (__ldg(first + mid) <= i) {
+            lo = mid;
+        } else {
+            hi = mid - 1;
+        }
+    }
+    return lo;
+}
+
+// Camera paths of every segment of a multi-job wave (grid-stride, so one grid size serves any
+// wave and the launch can be replayed from a graph).
+__global__ void __launch_bounds__(256) init_batch_kernel(KernelArgs a) {
+    const WaveDesc* w        = a.wave;
+    const uint32_t  n        = w->count;
+    const uint32_t  segments = w->segments;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t     k     = find_segment(w->first_path, segments, i);
+        const WaveSegment& g     = w->seg[k];
+        const uint32_t     local = i - g.first_path;
+        const uint32_t     area  = g.w * g.h;
+        const uint32_t     s     = local / area;
+        const uint32_t     r     = local - s * area;
+        const uint32_t     ry    = r / g.w;
+        Pcg32              rng;
+        const CameraRay    ray = camera_sample(g.scene.camera, g.x0 + (r - ry * g.w), g.y0 + ry,
+                                               g.s0 + s, g.width, g.height, g.seed, rng);
+        init_path(a, i, rng, ray.origin, ray.direction, ray.minimum, ray.maximum);
+        a.st.segment[i] = k;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        a.q.counters[0].ext = n;
+        atomicAdd(a.q.stats + kStatPaths, static_cast<unsigned long long>(n));
     }
 }
 
@@ -154,29 +239,33 @@ __global__ void init_rays_kernel(KernelArgs a, WaveInit w) {
 // Nearest hit of one extension ray, its material bin (or kNone) and, with media, the
 // free-flight sample over the hit interval.
 template <bool MEDIA>
-__device__ __forceinline__ uint32_t extend_item(const KernelArgs& a, uint32_t path, TraceCounters& tc,
-                                                unsigned& error) {
+__device__ __forceinline__ uint32_t extend_item(const KernelArgs& a, const DeviceScene& s, uint32_t path,
+                                                bool sorted, TraceCounters& tc, unsigned& error) {
     const float4 o4 = a.st.ray_o[path];
     const float4 d4 = a.st.ray_d[path];
     RayQuery     q;
     q.init(xyz(o4), xyz(d4));
-    const TraceResult r    = trace<false>(a.scene, q, o4.w, d4.w, tc, error);
+    const TraceResult r    = trace<false>(s, q, o4.w, d4.w, tc, error);
     uint32_t          kind = 0;
     if (r.slot != kNone) {
         a.st.hit[path] = make_float4(r.t, __fdiv_rn(r.a, r.det), __fdiv_rn(r.b, r.det),
                                      __fdiv_rn(r.c, r.det));
-        kind = (__float_as_uint(__ldg(a.scene.tris + 3 * static_cast<size_t>(r.slot) + 1).w) >> 8) & 0xffu;
+        if (sorted) {
+            kind = (__float_as_uint(__ldg(s.tris + 3 * static_cast<size_t>(r.slot) + 1).w) >> 8) & 0xffu;
+        }
     }
     a.st.hit_slot[path] = r.slot;
+    // Surface bins only group paths by material for the shading launch; unsorted, every
+    // surface hit goes to the first.
     uint32_t key        = r.slot == kNone ? kBinMiss : kBinDiffuse + kind;
-    if (MEDIA && a.scene.medium_count > 0) {
+    if (MEDIA && s.medium_count > 0) {
         // MediumField::sample over [minimum, hit ? distance : maximum]
         // (src/render/path_tracer.cpp:303-310).
         Pcg32  rng   = load_rng(a.st, path);
         float4 beta4 = a.st.beta[path];
         bool   scattered;
         float  scatter_t = 0, g = 0;
-        const f3 w = field_sample(a.scene, xyz(o4), xyz(d4), o4.w, r.slot != kNone ? r.t : d4.w, rng,
+        const f3 w = field_sample(s, xyz(o4), xyz(d4), o4.w, r.slot != kNone ? r.t : d4.w, rng,
                                   scattered, scatter_t, g, error);
         f3 beta = xyz(beta4) * w;
         store_rng(a.st, path, rng);
@@ -197,20 +286,20 @@ __device__ __forceinline__ uint32_t extend_item(const KernelArgs& a, uint32_t pa
 // Any hit of one shadow segment; adds the contribution (times the media transmittance) when
 // the segment is clear.
 template <bool MEDIA>
-__device__ __forceinline__ void shadow_item(const KernelArgs& a, uint32_t path, TraceCounters& tc,
-                                            unsigned& error) {
+__device__ __forceinline__ void shadow_item(const KernelArgs& a, const DeviceScene& s, uint32_t path,
+                                            TraceCounters& tc, unsigned& error) {
     const float4 o4 = a.st.shadow_o[path];
     const float4 d4 = a.st.shadow_d[path];
     RayQuery     q;
     q.init(xyz(o4), xyz(d4));
-    const TraceResult r = trace<true>(a.scene, q, 0.0f, o4.w, tc, error);
+    const TraceResult r = trace<true>(s, q, 0.0f, o4.w, tc, error);
     if (a.occluded_out) {
         a.occluded_out[path] = r.slot != kNone ? 1 : 0;
     }
     if (r.slot == kNone) {
         f3 c = xyz(a.st.shadow_c[path]);
-        if (MEDIA && a.scene.medium_count > 0) {
-            c = c * field_transmittance(a.scene, xyz(o4), xyz(d4), 0.0f, o4.w);
+        if (MEDIA && s.medium_count > 0) {
+            c = c * field_transmittance(s, xyz(o4), xyz(d4), 0.0f, o4.w);
         }
         const float4 L      = a.st.radiance[path];
         a.st.radiance[path] = make_float4(L.x + c.x, L.y + c.y, L.z + c.z, 0);
@@ -221,13 +310,15 @@ __device__ __forceinline__ void shadow_item(const KernelArgs& a, uint32_t path, 
 // then the shadow segments the previous bounce's shading queued (their contributions land
 // before this bounce's shading adds emission, the reference's accumulation order). Warps fetch
 // 32 consecutive items, so only the warp at the boundary mixes the two kinds. 8 resident blocks
-// per SM (<= 64 registers): the traversal is latency bound and more warps hide it.
-template <bool MEDIA>
+// per SM (<= 64 registers): the traversal is latency bound and more warps hide it. In a
+// multi-job wave (BATCH) every path finds its scene through its segment.
+template <bool MEDIA, bool BATCH>
 __global__ void __launch_bounds__(128, 8) trace_kernel(KernelArgs a) {
     BounceCounters* ctr      = a.q.counters + a.bounce;
     const uint32_t  n_ext    = ctr->ext;
     const uint32_t  n_shadow = a.bounce > 0 ? a.q.counters[a.bounce - 1].shadow : 0;
     const uint32_t  total    = n_ext + n_shadow;
+    const bool      sorted   = !BATCH || n_ext >= a.wave->sort_threshold;
     const uint32_t* in       = a.q.ext[a.bounce & 1];
     TraceCounters   tc_ext{0, 0}, tc_shadow{0, 0};
     unsigned        error = 0;
@@ -244,11 +335,16 @@ __global__ void __launch_bounds__(128, 8) trace_kernel(KernelArgs a) {
         const uint32_t i    = base + lane;
         uint32_t       key  = kNone;
         uint32_t       path = 0;
-        if (i < n_ext) {
-            path = in[i];
-            key  = extend_item<MEDIA>(a, path, tc_ext, error);
-        } else if (i < total) {
-            shadow_item<MEDIA>(a, a.q.shadow[i - n_ext], tc_shadow, error);
+        if (i < total) {
+            path                 = i < n_ext ? in[i] : a.q.shadow[i - n_ext];
+            const WaveSegment* g = segment_of<BATCH>(a, path);
+            unsigned           e = 0;
+            if (i < n_ext) {
+                key = extend_item<MEDIA>(a, scene_of<BATCH>(a, g), path, sorted, tc_ext, e);
+            } else {
+                shadow_item<MEDIA>(a, scene_of<BATCH>(a, g), path, tc_shadow, e);
+            }
+            note_error<BATCH>(g, e, error);
         }
         if (base < n_ext) {
             warp_append(key, path, ctr->bins, a.q.bins, a.capacity);
@@ -298,10 +394,12 @@ struct ShadeStats {
     uint32_t shadow_rays = 0, scattering = 0, roulette = 0, medium = 0;
 };
 
+template <bool BATCH>
 __device__ ShadeResult shade_surface(const KernelArgs& a, uint32_t path, int bin, ShadeStats& stats,
                                      unsigned& error) {
-    const DeviceScene&      s     = a.scene;
-    const IntegratorParams& p     = a.p;
+    const WaveSegment*      g     = segment_of<BATCH>(a, path);
+    const DeviceScene&      s     = scene_of<BATCH>(a, g);
+    const IntegratorParams& p     = params_of<BATCH>(a, g);
     const uint32_t          depth = a.bounce;
     const float4            d4    = a.st.ray_d[path];
     const f3                dir   = xyz(d4);
@@ -466,6 +564,7 @@ __device__ ShadeResult shade_surface(const KernelArgs& a, uint32_t path, int bin
     return out;
 }
 
+template <bool BATCH>
 __global__ void __launch_bounds__(128) shade_kernel(KernelArgs a) {
     BounceCounters* ctr = a.q.counters + a.bounce;
     uint32_t        prefix[kBinCount + 1];
@@ -490,7 +589,9 @@ __global__ void __launch_bounds__(128) shade_kernel(KernelArgs a) {
                 ++bin;
             }
             path                 = a.q.bins[bin * static_cast<size_t>(a.capacity) + (i - prefix[bin])];
-            const ShadeResult r  = shade_surface(a, path, bin, stats, error);
+            unsigned          e  = 0;
+            const ShadeResult r  = shade_surface<BATCH>(a, path, bin, stats, e);
+            note_error<BATCH>(segment_of<BATCH>(a, path), e, error);
             ext_key              = r.continue_path ? 0u : kNone;
             shadow_key           = r.shadow ? 0u : kNone;
         }
@@ -541,6 +642,57 @@ __global__ void resolve_kernel(const float4* radiance, uint32_t x0, uint32_t y0,
     }
     accumulator[2 * pixel]     = sum;
     accumulator[2 * pixel + 1] = comp;
+}
+
+// Multi-job resolve: every pixel of every segment adds its ns samples to its job's accumulator
+// in sample order (continuing the job's earlier samples; a segment starting at sample 0 starts
+// from zero), and a pixel whose last sample this is gets its mean written to the job's image with
+// the overflow check. Same arithmetic as resolve_kernel + finalize_kernel, so a job's image does
+// not depend on which wave carried which of its samples.
+__global__ void __launch_bounds__(256) resolve_batch_kernel(const float4* radiance, const WaveDesc* w,
+                                                            unsigned* error) {
+    const uint32_t n        = w->pixels;
+    const uint32_t segments = w->segments;
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        const uint32_t     k     = find_segment(w->first_pixel, segments, p);
+        const WaveSegment& g     = w->seg[k];
+        const uint32_t     r     = p - __ldg(w->first_pixel + k);
+        const uint32_t     area  = g.w * g.h;
+        const uint32_t     ry    = r / g.w;
+        const size_t       pixel = static_cast<size_t>(g.y0 + ry) * g.width + g.x0 + (r - ry * g.w);
+        float4 sum  = make_float4(0, 0, 0, 0);
+        float4 comp = make_float4(0, 0, 0, 0);
+        if (g.s0 > 0) {
+            sum  = g.accumulator[2 * pixel];
+            comp = g.accumulator[2 * pixel + 1];
+        }
+        bool bad = false;
+        for (uint32_t s = 0; s < g.ns; ++s) {
+            const float4 v = radiance[g.first_path + static_cast<size_t>(s) * area + r];
+            bad |= !(isfinite(v.x) && isfinite(v.y) && isfinite(v.z)) || v.x < 0 || v.y < 0 || v.z < 0;
+            neumaier(sum.x, comp.x, v.x);
+            neumaier(sum.y, comp.y, v.y);
+            neumaier(sum.z, comp.z, v.z);
+        }
+        unsigned e = bad ? kErrorRadiance : 0u;
+        g.accumulator[2 * pixel]     = sum;
+        g.accumulator[2 * pixel + 1] = comp;
+        if (g.s0 + g.ns == g.spp) {
+            const float count = static_cast<float>(g.spp);
+            const float cr = (sum.x + comp.x) / count, cg = (sum.y + comp.y) / count,
+                        cb = (sum.z + comp.z) / count;
+            if (!(isfinite(cr) && isfinite(cg) && isfinite(cb))) {
+                e |= kErrorOverflow;
+            }
+            g.rgb[3 * pixel]     = cr;
+            g.rgb[3 * pixel + 1] = cg;
+            g.rgb[3 * pixel + 2] = cb;
+        }
+        if (e) {
+            atomicOr(g.error, e);
+            atomicOr(error, e);
+        }
+    }
 }
 
 // Pixel mean and the overflow check of PathTracer::render (src/render/path_tracer.cpp:527-534).
@@ -600,11 +752,11 @@ LaunchShape& launch_shape() {
         int sms = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, current);
         int per = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, trace_kernel<false>, 128, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, trace_kernel<false, false>, 128, 0);
         shape.trace_blocks[0] = sms * std::max(1, per);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, trace_kernel<true>, 128, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, trace_kernel<true, false>, 128, 0);
         shape.trace_blocks[1] = sms * std::max(1, per);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, shade_kernel, 128, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, shade_kernel<false>, 128, 0);
         shape.shade_blocks = sms * std::max(1, per);
         device = current;
     }
@@ -648,6 +800,7 @@ std::shared_ptr<Workspace> allocate_workspace(size_t capacity, uint32_t max_boun
     const size_t o_so = field(capacity * sizeof(float4));
     const size_t o_sd = field(capacity * sizeof(float4));
     const size_t o_sc = field(capacity * sizeof(float4));
+    const size_t o_seg = field(capacity * sizeof(uint32_t));
     const size_t o_e0 = field(capacity * sizeof(uint32_t));
     const size_t o_e1 = field(capacity * sizeof(uint32_t));
     const size_t o_bins = field(capacity * kBinCount * sizeof(uint32_t));
@@ -676,6 +829,7 @@ std::shared_ptr<Workspace> allocate_workspace(size_t capacity, uint32_t max_boun
     ws->state.shadow_o      = reinterpret_cast<float4*>(base + o_so);
     ws->state.shadow_d      = reinterpret_cast<float4*>(base + o_sd);
     ws->state.shadow_c      = reinterpret_cast<float4*>(base + o_sc);
+    ws->state.segment       = reinterpret_cast<uint32_t*>(base + o_seg);
     ws->queues.ext[0]       = reinterpret_cast<uint32_t*>(base + o_e0);
     ws->queues.ext[1]       = reinterpret_cast<uint32_t*>(base + o_e1);
     ws->queues.bins         = reinterpret_cast<uint32_t*>(base + o_bins);
@@ -797,6 +951,7 @@ void Engine::run_wave(const Scene& scene, const IntegratorParams& params, const 
     a.capacity = static_cast<uint32_t>(ws.capacity);
     a.bounce   = 0;
     a.occluded_out = nullptr;
+    a.wave         = nullptr;
     MR_CUDA(cudaMemsetAsync(ws.queues.counters, 0, (params.maximum_depth + 2) * sizeof(BounceCounters),
                             stream));
     const unsigned blocks = (init.count + 127) / 128;
@@ -830,16 +985,16 @@ void Engine::run_wave(const Scene& scene, const IntegratorParams& params, const 
         // The first shadow rays (queued by bounce 0's shading) are traced with bounce 1.
         a.occluded_out = bounce == 1 && init.capture ? init.capture->occluded : nullptr;
         if (media) {
-            trace_kernel<true><<<shape.trace_blocks[1], 128, 0, stream>>>(a);
+            trace_kernel<true, false><<<shape.trace_blocks[1], 128, 0, stream>>>(a);
         } else {
-            trace_kernel<false><<<shape.trace_blocks[0], 128, 0, stream>>>(a);
+            trace_kernel<false, false><<<shape.trace_blocks[0], 128, 0, stream>>>(a);
         }
         a.occluded_out = nullptr;
         if (timed) {
             cudaEventRecord(e1, stream);
             events.emplace_back(e0, e1);
         }
-        shade_kernel<<<shape.shade_blocks, 128, 0, stream>>>(a);
+        shade_kernel<false><<<shape.shade_blocks, 128, 0, stream>>>(a);
         if (bounce == 0 && init.capture) {
             capture_shadow_kernel<<<(init.count + 127) / 128, 128, 0, stream>>>(a, init.capture->rays,
                                                                                 init.capture->has_shadow);
@@ -865,6 +1020,51 @@ void Engine::run_wave(const Scene& scene, const IntegratorParams& params, const 
         timing.counted.bounds_tests += (after[0] - before[0]) + (after[2] - before[2]);
         timing.counted.triangle_tests += (after[1] - before[1]) + (after[3] - before[3]);
     }
+}
+
+void Engine::batch_occupancy(int& trace_blocks_per_sm, int& shade_blocks_per_sm) {
+    int a = 0, b = 0, c = 0;
+    MR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, trace_kernel<false, true>, 128, 0));
+    MR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, trace_kernel<true, true>, 128, 0));
+    MR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, shade_kernel<true>, 128, 0));
+    trace_blocks_per_sm = std::max(1, std::min(a, b));
+    shade_blocks_per_sm = std::max(1, c);
+}
+
+void Engine::enqueue_batch_paths(const WaveDesc* wave, uint32_t maximum_depth, bool media,
+                                 const BatchShape& shape, Workspace& ws, cudaStream_t stream) {
+    if (maximum_depth + 1 > ws.max_bounces || !ws.state.segment) {
+        fail(MR_LENGTH_ERROR, "Wave exceeds the workspace capacity");
+    }
+    int device = 0, sms = 0;
+    MR_CUDA(cudaGetDevice(&device));
+    MR_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    KernelArgs a{};
+    a.st           = ws.state;
+    a.q            = ws.queues;
+    a.capacity     = static_cast<uint32_t>(ws.capacity);
+    a.occluded_out = nullptr;
+    a.wave         = wave;
+    MR_CUDA(cudaMemsetAsync(ws.queues.counters, 0, (maximum_depth + 2) * sizeof(BounceCounters), stream));
+    init_batch_kernel<<<sms * 8, 256, 0, stream>>>(a);
+    for (uint32_t bounce = 0; bounce <= maximum_depth; ++bounce) {
+        a.bounce = bounce;
+        if (media) {
+            trace_kernel<true, true><<<shape.trace_blocks, 128, 0, stream>>>(a);
+        } else {
+            trace_kernel<false, true><<<shape.trace_blocks, 128, 0, stream>>>(a);
+        }
+        shade_kernel<true><<<shape.shade_blocks, 128, 0, stream>>>(a);
+    }
+    MR_CUDA(cudaGetLastError());
+}
+
+void Engine::enqueue_batch_resolve(const WaveDesc* wave, Workspace& ws, cudaStream_t stream) {
+    int device = 0, sms = 0;
+    MR_CUDA(cudaGetDevice(&device));
+    MR_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    resolve_batch_kernel<<<sms * 8, 256, 0, stream>>>(ws.state.radiance, wave, ws.queues.error);
+    MR_CUDA(cudaGetLastError());
 }
 
 void render_tile(const Scene& scene, const IntegratorParams& params, const mr_render_settings& render,

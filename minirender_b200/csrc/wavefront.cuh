@@ -48,6 +48,37 @@ struct IntegratorParams {
     uint32_t roulette_depth;
 };
 
+// One job's share of a multi-job wave: a pixel rectangle x sample range of one render, with
+// everything the kernels need to trace it (the job's scene, integrator settings and buffers).
+struct WaveSegment {
+    DeviceScene      scene;
+    IntegratorParams p;
+    uint32_t         x0, y0, w, h;      // pixel rectangle
+    uint32_t         s0, ns;            // samples s0 .. s0+ns, sample-major path slots
+    uint32_t         width, height, spp;
+    uint32_t         first_path;        // wave slot of the segment's first path
+    uint64_t         seed;
+    float4*          accumulator;       // the job's (sum, compensation) per pixel
+    float*           rgb;               // the job's image; pixels whose last sample resolves here
+    unsigned*        error;             // the job's error word
+};
+
+constexpr uint32_t kMaxSegments = 1024;
+
+// Device descriptor of a multi-job wave. Segments are sorted by first_path; first_path[] and
+// first_pixel[] hold count+1 prefix entries so kernels find a path's or pixel's segment by
+// binary search.
+struct WaveDesc {
+    uint32_t    count;           // paths in the wave
+    uint32_t    segments;
+    uint32_t    pixels;          // resolve index space: sum of w*h over segments
+    uint32_t    sort_threshold;  // queues shorter than this are not sorted by material
+    uint32_t    first_path[kMaxSegments + 1];
+    uint32_t    first_pixel[kMaxSegments + 1];
+    uint32_t    pad[2];
+    WaveSegment seg[kMaxSegments];
+};
+
 // Structure-of-arrays path state of `capacity` paths (one 16-byte record per field).
 struct PathState {
     ulonglong2* rng;       // PCG state, increment
@@ -62,6 +93,7 @@ struct PathState {
     float4*     shadow_o;  // shadow origin, segment limit
     float4*     shadow_d;  // shadow direction
     float4*     shadow_c;  // unoccluded contribution
+    uint32_t*   segment;   // multi-job waves: the path's wave segment
 };
 
 struct Queues {
@@ -115,12 +147,34 @@ struct WaveInit {
     ShadowCapture*  capture;          // optional diagnostics (host struct of device pointers)
 };
 
+// Grid sizes of the persistent kernels of a multi-job wave (blocks of 128 threads).
+struct BatchShape {
+    int trace_blocks = 0;
+    int shade_blocks = 0;
+};
+
 class Engine {
   public:
     // Renders one wave on `stream`: initialises `count` paths, runs up to maximum_depth + 1
     // bounces. Path radiance stays in ws.state.radiance (slot order).
     static void run_wave(const Scene& scene, const IntegratorParams& params, const WaveInit& init,
                          Workspace& ws, cudaStream_t stream);
+
+    // Enqueues the paths of one multi-job wave whose descriptor is already in device memory
+    // (`wave`): camera paths of every segment and up to maximum_depth + 1 bounces; radiance stays
+    // per path. The launch sequence depends only on its arguments, so it can be captured once in
+    // a CUDA graph and replayed for every wave of the same depth.
+    static void enqueue_batch_paths(const WaveDesc* wave, uint32_t maximum_depth, bool media,
+                                    const BatchShape& shape, Workspace& ws, cudaStream_t stream);
+
+    // Enqueues the per-pixel resolve of a wave's radiance into each job's accumulator and image.
+    static void enqueue_batch_resolve(const WaveDesc* wave, Workspace& ws, cudaStream_t stream);
+
+    // Largest grids the batch kernels can keep resident (blocks per SM at 128 threads).
+    static void batch_occupancy(int& trace_blocks_per_sm, int& shade_blocks_per_sm);
+
+    // Kernel launches of one wave (paths + resolve).
+    static uint64_t batch_wave_launches(uint32_t maximum_depth) { return 2ull + 2ull * (maximum_depth + 1); }
 };
 
 // Workspace pool (per device).

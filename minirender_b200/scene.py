@@ -526,3 +526,21 @@ def job_scene(triangles: int, seed: int) -> SceneDocument:
                                        Transform(c, tuple(rng.uniform(0, 360, 3).tolist()),
                                                  (radius, radius, radius))))
     return doc
+
+
+def job_table(count: int = 256, seed: int = 3) -> list[dict]:
+    """The uneven job mix of the batching and serving workloads, seeded: triangle count
+    log-uniform in [10k, 500k], square resolution with pixel count log-uniform in
+    [128^2, 1024^2], samples per pixel log-uniform in [4, 256], maximum depth uniform in
+    {4, ..., 12}, render seed per job."""
+    rng = np.random.default_rng(seed)
+    jobs = []
+    for i in range(count):
+        triangles = int(round(np.exp(rng.uniform(np.log(10_000), np.log(500_000)))))
+        side = int(round(np.exp(rng.uniform(np.log(128), np.log(1024)))))
+        spp = int(round(np.exp(rng.uniform(np.log(4), np.log(256)))))
+        depth = int(rng.integers(4, 13))
+        jobs.append({"triangles": triangles, "width": side, "height": side,
+                     "samples_per_pixel": spp, "maximum_depth": depth,
+                     "scene_seed": seed * 100_003 + i, "render_seed": i + 1})
+    return jobs
