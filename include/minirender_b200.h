@@ -290,6 +290,23 @@ size_t mr_last_error(char* buffer, size_t capacity);
  * (src/render/light.cpp:340-407) and the MediumField (src/render/medium.cpp:228-231). */
 mr_status mr_scene_create(const mr_scene_desc* desc, const mr_bvh_desc* bvh, mr_scene** scene);
 
+/* Builder options. No reference counterpart: the reference bins whole triangles only. */
+typedef struct mr_build_settings {
+    uint32_t split_references; /* nonzero: early split clipping. A triangle whose box area exceeds
+                                  split_factor x the mean triangle box area enters the build once
+                                  per nonempty cell of a grid over its box, with the clipped
+                                  bounds. Hits, images and statistics of paths are unchanged (the
+                                  same triangles are tested); the tree, its SAH cost and its leaf
+                                  slots differ from the reference builder's. */
+    float    split_factor;     /* 0 = 16 */
+    uint64_t max_references;   /* cap on leaf slots; 0 = max(2 x triangles, triangles + 65536) */
+} mr_build_settings;
+
+/* mr_scene_create with builder options (`build` NULL = mr_scene_create). A scene built with
+ * split references cannot be exported in the reference layout (MR_LOGIC_ERROR). */
+mr_status mr_scene_create_with(const mr_scene_desc* desc, const mr_bvh_desc* bvh,
+                               const mr_build_settings* build, mr_scene** scene);
+
 /* Releases every device and host resource of the scene. */
 mr_status mr_scene_destroy(mr_scene* scene);
 

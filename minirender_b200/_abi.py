@@ -97,6 +97,11 @@ class BvhDesc(C.Structure):
                 ("order", C.POINTER(C.c_uint32)), ("primitive_count", C.c_uint32)]
 
 
+class BuildSettings(C.Structure):
+    _fields_ = [("split_references", C.c_uint32), ("split_factor", C.c_float),
+                ("max_references", C.c_uint64)]
+
+
 class IntegratorSettings(C.Structure):
     _fields_ = [("mode", C.c_uint32), ("maximum_depth", C.c_uint32),
                 ("russian_roulette", C.c_uint32), ("roulette_depth", C.c_uint32)]
@@ -205,6 +210,7 @@ SIGNATURES = {
     "mr_abi_version": (C.c_uint32, []),
     "mr_last_error": (C.c_size_t, [C.c_char_p, C.c_size_t]),
     "mr_scene_create": (C.c_int, [P(SceneDesc), P(BvhDesc), P(VP)]),
+    "mr_scene_create_with": (C.c_int, [P(SceneDesc), P(BvhDesc), P(BuildSettings), P(VP)]),
     "mr_scene_destroy": (C.c_int, [VP]),
     "mr_scene_bvh_statistics": (C.c_int, [VP, P(BvhStatistics)]),
     "mr_scene_sah_cost": (C.c_int, [VP, P(C.c_double)]),

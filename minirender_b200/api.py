@@ -87,15 +87,18 @@ class Scene:
     """A snapshot uploaded to the current CUDA device with its BVH, lights and media
     (the construction half of PathTracer, src/render/path_tracer.cpp:244-253)."""
 
-    def __init__(self, snapshot: Snapshot | SceneDocument, bvh: _abi.BvhDesc | None = None):
+    def __init__(self, snapshot: Snapshot | SceneDocument, bvh: _abi.BvhDesc | None = None,
+                 split_references: bool = False, split_factor: float = 0.0,
+                 max_references: int = 0):
         self.lib = load_library()
         if isinstance(snapshot, SceneDocument):
             snapshot = snapshot.snapshot()
         self.snapshot = snapshot
         handle = C.c_void_p()
-        check(self.lib.mr_scene_create(snapshot.desc_pointer(),
-                                       C.pointer(bvh) if bvh is not None else None,
-                                       C.byref(handle)), self.lib)
+        build = _abi.BuildSettings(int(split_references), split_factor, max_references)
+        check(self.lib.mr_scene_create_with(snapshot.desc_pointer(),
+                                            C.pointer(bvh) if bvh is not None else None,
+                                            C.byref(build), C.byref(handle)), self.lib)
         self.handle = handle
 
     def close(self):

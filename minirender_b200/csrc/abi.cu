@@ -458,6 +458,18 @@ mr_status mr_scene_create(const mr_scene_desc* desc, const mr_bvh_desc* bvh, mr_
     });
 }
 
+mr_status mr_scene_create_with(const mr_scene_desc* desc, const mr_bvh_desc* bvh,
+                               const mr_build_settings* build, mr_scene** scene) {
+    return guarded([&] {
+        require(desc != nullptr && scene != nullptr, "Scene descriptor or output is null");
+        require(!(bvh && build && build->split_references),
+                "Split references apply to the GPU builder, not to an imported tree");
+        auto s  = std::make_unique<mr_scene>();
+        s->impl = create_scene(*desc, bvh, build);
+        *scene  = s.release();
+    });
+}
+
 mr_status mr_scene_destroy(mr_scene* scene) {
     return guarded([&] { delete scene; });
 }
@@ -476,6 +488,9 @@ mr_status mr_scene_export_bvh(const mr_scene* scene, mr_bvh_node* nodes, uint32_
         const Scene&   s = scene_of(scene);
         const uint32_t n = static_cast<uint32_t>(s.ref_nodes.count);
         const uint32_t p = s.d.primitive_count;
+        if (s.references != p) {
+            fail(MR_LOGIC_ERROR, "A tree with split references has no reference-layout export");
+        }
         if (node_count) {
             *node_count = n;
         }

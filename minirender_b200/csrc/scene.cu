@@ -373,7 +373,8 @@ void validate_imported(const mr_bvh_desc& b, uint32_t prims) {
 
 }  // namespace
 
-std::unique_ptr<Scene> create_scene(const mr_scene_desc& desc, const mr_bvh_desc* bvh) {
+std::unique_ptr<Scene> create_scene(const mr_scene_desc& desc, const mr_bvh_desc* bvh,
+                                    const mr_build_settings* build) {
     int device_count = 0;
     if (cudaGetDeviceCount(&device_count) != cudaSuccess || device_count == 0) {
         fail(MR_CUDA_ERROR, "No CUDA device is available");
@@ -530,15 +531,37 @@ std::unique_ptr<Scene> create_scene(const mr_scene_desc& desc, const mr_bvh_desc
             scene->statistics.leaves        = leaves;
             scene->statistics.maximum_depth = depth;
         } else {
-            BuildResult built = build_bvh_device(lo.ptr, hi.ptr, centroid.ptr, prims, stream);
+            SplitReferences split;
+            if (build && build->split_references) {
+                const float    factor = build->split_factor > 0 ? build->split_factor : 16.0f;
+                const uint64_t cap    = build->max_references
+                                            ? build->max_references
+                                            : std::max<uint64_t>(2ull * prims, prims + 65536ull);
+                require(std::isfinite(factor) && cap >= prims && cap <= 0xFFFFFFFFull,
+                        "Split settings need a finite factor and a reference cap of at least the "
+                        "triangle count");
+                split = split_references(world.ptr, lo.ptr, hi.ptr, prims, factor, cap, stream);
+            }
+            const uint32_t refs  = split.count ? split.count : prims;
+            BuildResult    built = split.count
+                                       ? build_bvh_device(split.lo.ptr, split.hi.ptr, split.centroid.ptr, refs, stream)
+                                       : build_bvh_device(lo.ptr, hi.ptr, centroid.ptr, prims, stream);
+            if (split.count) {
+                map_order_to_primitives(built.order.ptr, split.prim.ptr, refs, stream);
+            }
             ref_nodes             = std::move(built.nodes);
             ref_order             = std::move(built.order);
             node_count            = built.node_count;
             scene->statistics.leaves        = built.leaves;
             scene->statistics.maximum_depth = built.maximum_depth;
             scene->build_seconds  = built.seconds;
+            scene->references     = refs;
         }
     }
+    if (scene->references == 0) {
+        scene->references = prims;
+    }
+    const uint32_t slots = scene->references;
     scene->statistics.triangles = prims;
     scene->statistics.nodes     = node_count;
     lo.release();
@@ -583,8 +606,8 @@ std::unique_ptr<Scene> create_scene(const mr_scene_desc& desc, const mr_bvh_desc
             }
             wide_count = base;
         }
-        scene->tris.allocate(3ull * prims);
-        gather_triangles_kernel<<<(prims + 255) / 256, 256, 0, stream>>>(world.ptr, ref_order.ptr, prims,
+        scene->tris.allocate(3ull * slots);
+        gather_triangles_kernel<<<(slots + 255) / 256, 256, 0, stream>>>(world.ptr, ref_order.ptr, slots,
                                                                          scene->tris.ptr);
         mark_leaf_end_kernel<<<(node_count + 255) / 256, 256, 0, stream>>>(ref_nodes.ptr, node_count,
                                                                            scene->tris.ptr);

@@ -62,13 +62,28 @@ struct Scene {
     DeviceBuffer<mr_bvh_node> ref_nodes;
     DeviceBuffer<uint32_t>    ref_order;
     mr_bvh_statistics        statistics{};
+    uint32_t                 references    = 0;  // leaf slots; above the triangle count when split
     double                   build_seconds = 0;
     double                   sah_cost      = 0;
     size_t                   device_bytes  = 0;
 };
 
-// Scene construction (scene.cu).
-std::unique_ptr<Scene> create_scene(const mr_scene_desc& desc, const mr_bvh_desc* bvh);
+// Scene construction (scene.cu). `build` (optional) selects split references for the builder.
+std::unique_ptr<Scene> create_scene(const mr_scene_desc& desc, const mr_bvh_desc* bvh,
+                                    const mr_build_settings* build = nullptr);
+
+// Early split clipping (split.cu): references (bounds, centroid, triangle) of the triangles,
+// oversized ones entered once per nonempty cell of a grid over their box. count == 0 when no
+// triangle is worth splitting (build over the triangles themselves).
+struct SplitReferences {
+    DeviceBuffer<float4>   lo, hi, centroid;
+    DeviceBuffer<uint32_t> prim;
+    uint32_t               count = 0;
+};
+SplitReferences split_references(const float4* world, const float4* lo, const float4* hi, uint32_t prims,
+                                  float factor, uint64_t max_references, cudaStream_t stream);
+// Replaces the reference indices of a built leaf order by their triangles.
+void map_order_to_primitives(uint32_t* order, const uint32_t* prim, uint32_t count, cudaStream_t stream);
 
 // GPU binned-SAH builder (builder.cu): from per-primitive FP32 bounds and centroids on the
 // device to a reference-layout tree (DFS-independent node numbering, root at index 0).

@@ -1,0 +1,81 @@
+"""Split references (early split clipping) change the tree, not the answers: nearest hits and
+occlusion are those of the unsplit tree except t-ties (coplanar faces hit at the same FP64
+distance, where FP32 rounding and traversal order pick the winner, the class the parity tests
+document), images and path statistics other than the traversal counters are bitwise the same
+for scenes without such ties in view, and the SAH cost of a room around detailed objects drops."""
+
+import numpy as np
+import pytest
+
+from minirender_b200 import scene as sc
+
+pytestmark = pytest.mark.gpu
+
+from tests.test_gpu_parity import classify_mismatch  # noqa: E402
+
+
+@pytest.fixture(scope="module")
+def api():
+    from minirender_b200 import api as a
+    return a
+
+
+def rays_in_box(n, seed, lo=-0.5, hi=0.5):
+    rng = np.random.default_rng(seed)
+    o = rng.uniform([lo, 0.0, lo], [hi, 1.0, hi], (n, 3)).astype(np.float32)
+    d = rng.normal(size=(n, 3))
+    d = (d / np.linalg.norm(d, axis=1, keepdims=True)).astype(np.float32)
+    return o, d
+
+
+@pytest.mark.parametrize("doc_factory", [lambda: sc.job_scene(40_000, 12), sc.cornell_box,
+                                         lambda: sc.job_scene(150_000, 5)])
+def test_split_tree_gives_identical_hits(api, doc_factory):
+    doc = doc_factory()
+    plain = api.Scene(doc.snapshot())
+    split = api.Scene(doc.snapshot(), split_references=True)
+    o, d = rays_in_box(200_000, 9)
+    ha, _ = plain.intersect(o, d, 0.0, np.inf)
+    hb, _ = split.intersect(o, d, 0.0, np.inf)
+    assert (ha["primitive"] != 0xFFFFFFFF).mean() > 0.8  # rays start inside a room open at the front
+    differ = np.nonzero((ha["primitive"] != hb["primitive"]) | (ha["distance"] != hb["distance"]))[0]
+    tris = doc.snapshot().world_triangles()
+    for i in differ:  # only ties: both triangles at the same FP64 distance
+        cls = classify_mismatch(tris, o[i].astype(np.float64), d[i].astype(np.float64), None,
+                                int(ha["primitive"][i]), int(hb["primitive"][i]))
+        assert cls == "tie", (i, ha[i], hb[i])
+    assert len(differ) <= 1e-4 * len(o)
+    same = np.setdiff1d(np.arange(len(o)), differ)
+    for key in ha.dtype.names:
+        np.testing.assert_array_equal(ha[key][same], hb[key][same])
+    oa, _ = plain.occluded(o, d, 0.0, 0.75)
+    ob, _ = split.occluded(o, d, 0.0, 0.75)
+    np.testing.assert_array_equal(oa, ob)
+    assert plain.statistics()["triangles"] == split.statistics()["triangles"]
+
+
+def test_split_tree_renders_identical_images_and_lower_cost(api):
+    doc = sc.job_scene(60_000, 21)
+    plain = api.Scene(doc.snapshot())
+    split = api.Scene(doc.snapshot(), split_references=True)
+    assert split.sah_cost() < 0.85 * plain.sah_cost()
+    settings = api.IntegratorSettings("mis", 10, True, 3)
+    render = api.RenderSettings(96, 72, 8, 4)
+    img_a, st_a = api.PathTracer(plain, settings).render(render)
+    img_b, st_b = api.PathTracer(split, settings).render(render)
+    np.testing.assert_array_equal(img_a, img_b)
+    for key in ("paths", "shadow_rays", "scattering_events", "roulette_terminations"):
+        assert st_a[key] == st_b[key]
+    assert st_b["bounds_tests"] < st_a["bounds_tests"]
+    with pytest.raises(api.MiniRenderError):
+        split.export_bvh()
+
+
+def test_unsplittable_scene_keeps_reference_tree(api):
+    doc = sc.sphere_field(20, 6.0, 3, subdivisions=2)
+    plain = api.Scene(doc.snapshot())
+    split = api.Scene(doc.snapshot(), split_references=True, split_factor=1e6)
+    assert split.sah_cost() == plain.sah_cost()
+    nodes_a, order_a, _ = plain.export_bvh()
+    nodes_b, order_b, _ = split.export_bvh()
+    np.testing.assert_array_equal(order_a, order_b)
