@@ -1,23 +1,33 @@
 #!/usr/bin/env python
-"""Throughput of the GPU offline path tracer on the 1M-triangle workload, in Msamples/s.
+"""Throughput of the GPU offline path tracer on the uneven job mix, in Msamples/s.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Workload: the procedural ~1M-triangle scene (200 displaced 4-subdivision icospheres in a 20^3 box
-on a ground quad, constant environment plus one directional light, thin lens with aperture 0.05
-and focus distance 10), 1920x1080, 64 samples per pixel, maximum depth 12, MIS, Russian roulette
-from depth 3. One step renders one full frame (132,710,400 camera samples). Synthetic, seeded.
+Workload: 256 seeded render jobs. Each job is a Cornell room (5 walls, two boxes, a ceiling
+light) filled with displaced icospheres up to its triangle count, drawn log-uniform in
+[10k, 500k]; square images with pixel count log-uniform in [128^2, 1024^2]; samples per pixel
+log-uniform in [4, 256]; maximum depth uniform in {4..12}; MIS, Russian roulette from depth 3.
+One step renders all 256 jobs (about 3.2 G camera samples). Synthetic: the scenes and the job
+table come from the package's seeded generators. Scenes are built with split references (the
+result-neutral builder option for rooms around detailed objects).
 
-Ours: the scene is resident in HBM (uploaded and BVH built once); `value` is samples of all ranks
-over the slowest rank's device time for K frames (CUDA events on the launching stream, barrier +
-synchronize on both sides, L2 flushed by a 256 MB write before every frame). `e2e` is the same
-metric through the public API from pinned host buffers: every step creates the scene (upload +
-GPU BVH build) and renders into a host image. Multi-GPU runs are weak-scaled: each rank renders
-its own frame (seed = rank + 1), no collective on the data path.
+Ours: the scenes are resident in HBM. `value` is the batched engine (mr_render_batch: jobs packed
+into shared waves, CUDA graphs, concurrent wave lanes, shape from the autotuner run beforehand on
+a calibration subset), camera samples of all ranks over the slowest rank's device time of K steps;
+device time comes from CUDA events the engine records on its own streams around each step. The
+inputs (scenes: tens of millions of triangles; path state: GBs) exceed L2, so no flush is added.
+Beside it, on the same jobs and scenes: the plain one-job-per-call path (mr_render_device per job,
+CUDA events on the caller's stream, kernel timing of the traversal kernel for the roofline), a
+serving run (Poisson arrivals at 50 jobs/s through the render server, 5% cancelled, p50/p99
+latency from submission to image in host memory), and the single 1M-triangle frame
+(1920x1080, 64 spp, depth 12). `e2e` repeats the step through the public API from pinned host
+memory: every step creates the 256 scenes (upload + GPU build) and renders them with images read
+back to host memory. Multi-GPU runs are weak-scaled: each rank renders its own copy of the job
+table with rank-specific render seeds; no collective on the data path.
 
-Reference (--impl reference): the CPU oracle's tile-parallel render (the reference algorithm
-restated; the reference itself does not build here) on the host cores, rank 0 only, each step a
-bounded band of rows of the same frame.
+Reference (--impl reference): the CPU oracle (the reference algorithm restated; the reference
+itself does not build here) on the host cores, rank 0 only, each step a bounded band of rows of
+four jobs spread over the table.
 """
 
 from __future__ import annotations
@@ -30,7 +40,6 @@ import statistics
 import subprocess
 import sys
 import tempfile
-import threading
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -38,33 +47,33 @@ sys.path.insert(0, ROOT)
 
 import numpy as np  # noqa: E402
 
-WIDTH, HEIGHT, SPP, DEPTH = 1920, 1080, 64, 12
 METRIC = "Msamples/s"
+JOBS = 256
+TABLE_SEED = 3
 FALLBACK_HBM_GBS = 6650.0
 BYTES_PER_BOUNDS_TEST = 24   # one FP32 AABB
 BYTES_PER_TRIANGLE_TEST = 36  # one FP32 triangle
+CPU_SAMPLE_JOBS = (0, 64, 128, 192)
+SERVE_RATE = 50.0             # jobs per second
+CANCEL_FRACTION = 0.05
 
 
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--steps", type=int, default=3)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--cpu-seconds", type=float, default=12.0,
                    help="target CPU time of the bounded CPU-baseline sample")
+    p.add_argument("--serve-seconds", type=float, default=8.0,
+                   help="length of the Poisson arrival window of the serving run")
     p.add_argument("--no-cpu-baseline", action="store_true")
-    # Profiling aids (ncu captures of a smaller frame); the defaults are the benchmark.
-    p.add_argument("--resolution", default=None, help="WxH override, e.g. 960x540")
-    p.add_argument("--spp", type=int, default=None)
     p.add_argument("--no-e2e", action="store_true")
-    args = p.parse_args()
-    global WIDTH, HEIGHT, SPP
-    if args.resolution:
-        WIDTH, HEIGHT = (int(v) for v in args.resolution.lower().split("x"))
-    if args.spp:
-        SPP = args.spp
-    return args
+    p.add_argument("--no-serve", action="store_true")
+    # Profiling aid (ncu captures): render only the first J jobs. The default is the benchmark.
+    p.add_argument("--jobs", type=int, default=JOBS)
+    return p.parse_args()
 
 
 def rank_info():
@@ -72,18 +81,25 @@ def rank_info():
             int(os.environ.get("LOCAL_RANK", 0)))
 
 
-def workload():
+def job_table(count):
     from minirender_b200 import scene as sc
-    return sc.large_scene()
+    return sc.job_table(JOBS, TABLE_SEED)[:count]
 
 
-def config(triangles):
-    return {"workload": "procedural-1M-triangles 1920x1080 64spp depth12 mis",
-            "triangles": triangles, "width": WIDTH, "height": HEIGHT, "spp": SPP,
-            "maximum_depth": DEPTH, "mode": "mis", "roulette_depth": 3,
-            "samples_per_frame": WIDTH * HEIGHT * SPP,
-            "l2": "256 MB write before every timed frame (included); per-frame path state "
-                  "~1.8 GB > L2"}
+def job_document(job):
+    from minirender_b200 import scene as sc
+    return sc.job_scene(job["triangles"], job["scene_seed"])
+
+
+def config(table, triangles):
+    return {"workload": f"uneven job mix: {len(table)} Cornell rooms with displaced icospheres, "
+                        "10k-500k triangles, 128^2-1024^2 px, 4-256 spp, depth 4-12, mis",
+            "jobs": len(table), "triangles_total": triangles,
+            "samples_per_step": sum(j["width"] * j["height"] * j["samples_per_pixel"] for j in table),
+            "job_table_seed": TABLE_SEED, "mode": "mis", "roulette_depth": 3,
+            "bvh": "GPU binned SAH with split references",
+            "l2": "no flush: scenes (tens of millions of triangles) and per-wave path state "
+                  "(GBs) exceed the 126 MB L2"}
 
 
 def measured_peak():
@@ -168,72 +184,157 @@ def cpu_threads():
     return max(1, min(hw - 1 if hw > 1 else 1, 32))
 
 
-def cpu_render_band(oracle_scene, rows, seed=1):
-    from minirender_b200 import _abi
-    rs = _abi.RenderSettings(WIDTH, HEIGHT, SPP, seed)
-    r0 = HEIGHT // 2 - rows // 2
-    t0 = time.perf_counter()
-    oracle_scene.render(rs, threads=cpu_threads(), rows=(r0, r0 + rows), statistics=False)
-    return time.perf_counter() - t0
+class CpuSample:
+    """A bounded CPU-oracle sample of the workload: a central band of rows of four jobs spread
+    over the table, each band sized for a share of a target CPU time."""
+
+    def __init__(self, table, target_seconds):
+        from minirender_b200 import _abi
+        from oracle import pyoracle
+        self.parts = []
+        self.build = 0.0
+        for k in CPU_SAMPLE_JOBS:
+            if k >= len(table):
+                continue
+            job = table[k]
+            t0 = time.perf_counter()
+            o = pyoracle.OracleScene(job_document(job).snapshot(),
+                                     pyoracle.integrator("mis", job["maximum_depth"], True, 3))
+            self.build += time.perf_counter() - t0
+            rs = _abi.RenderSettings(job["width"], job["height"], job["samples_per_pixel"],
+                                     job["render_seed"])
+            self.parts.append([o, rs, job, 1, k])
+        per_job = target_seconds / max(1, len(self.parts))
+        for part in self.parts:  # calibrate the band height per job
+            rows, elapsed = 1, self._band(part, 1)
+            while elapsed < 0.25 and rows < part[2]["height"]:
+                rows = min(part[2]["height"], rows * 4)
+                elapsed = self._band(part, rows)
+            part[3] = int(max(1, min(part[2]["height"], round(per_job * rows / max(elapsed, 1e-6)))))
+
+    @staticmethod
+    def _band(part, rows):
+        o, rs, job = part[0], part[1], part[2]
+        r0 = job["height"] // 2 - rows // 2
+        t0 = time.perf_counter()
+        o.render(rs, threads=cpu_threads(), rows=(r0, r0 + rows), statistics=False)
+        return time.perf_counter() - t0
+
+    def run(self):
+        seconds, samples = 0.0, 0
+        for part in self.parts:
+            seconds += self._band(part, part[3])
+            samples += part[3] * part[2]["width"] * part[2]["samples_per_pixel"]
+        return samples, seconds
+
+    def describe(self, samples, seconds):
+        bands = ", ".join(f"job {p[4]}: {p[3]} rows x {p[2]['width']} px x "
+                          f"{p[2]['samples_per_pixel']} spp" for p in self.parts)
+        return (f"central row bands ({bands}); {samples} samples in {seconds:.1f} s; oracle "
+                f"BVH builds {self.build:.1f} s single-threaded (not in the rate); host has "
+                f"{os.cpu_count()} hardware threads")
 
 
-def calibrated_rows(oracle_scene, target_seconds):
-    rows, elapsed = 1, cpu_render_band(oracle_scene, 1)
-    while elapsed < 0.5 and rows < HEIGHT:
-        rows = min(HEIGHT, rows * 4)
-        elapsed = cpu_render_band(oracle_scene, rows)
-    per_row = elapsed / rows
-    return int(max(1, min(HEIGHT, round(target_seconds / per_row))))
-
-
-def cpu_baseline(snapshot, target_seconds):
-    from oracle import pyoracle
-    t0 = time.perf_counter()
-    o = pyoracle.OracleScene(snapshot, pyoracle.integrator("mis", DEPTH, True, 3))
-    build = time.perf_counter() - t0
-    rows = calibrated_rows(o, target_seconds)
-    seconds = cpu_render_band(o, rows)
-    samples = rows * WIDTH * SPP
+def cpu_baseline(table, target_seconds):
+    sample = CpuSample(table, target_seconds)
+    samples, seconds = sample.run()
     return {"value": samples / seconds / 1e6, "unit": METRIC, "cores": cpu_threads(),
-            "kind": "port",
-            "sample": f"{rows} rows x 1920 px x 64 spp ({samples} samples) of the same frame, "
-                      f"central band, {seconds:.1f} s; BVH build {build:.2f} s single-threaded "
-                      f"(not in the rate); host has {os.cpu_count()} hardware threads"}
+            "kind": "port", "sample": sample.describe(samples, seconds)}
 
 
 def run_reference(args):
     rank, world, _ = rank_info()
     if rank != 0:
         return 0
-    from oracle import pyoracle
-    doc = workload()
-    snap = doc.snapshot()
-    o = pyoracle.OracleScene(snap, pyoracle.integrator("mis", DEPTH, True, 3))
-    total_budget = float(os.environ.get("BENCH_REFERENCE_SECONDS", 120.0))  # warmup + steps
-    rows = calibrated_rows(o, total_budget / max(1, args.steps + args.warmup))
+    table = job_table(args.jobs)
+    budget = float(os.environ.get("BENCH_REFERENCE_SECONDS", 120.0))  # warmup + steps
+    sample = CpuSample(table, budget / max(1, args.steps + args.warmup))
     for _ in range(args.warmup):
-        cpu_render_band(o, rows)
-    seconds = sum(cpu_render_band(o, rows) for _ in range(args.steps))
-    samples = rows * WIDTH * SPP * args.steps
+        sample.run()
+    samples, seconds = 0, 0.0
+    for _ in range(args.steps):
+        n, s = sample.run()
+        samples += n
+        seconds += s
     value = samples / seconds / 1e6
     line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * seconds / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": config(snap.triangle_count), "impl": "reference",
+            "config": config(table, sum(j["triangles"] for j in table)), "impl": "reference",
             "cpu_baseline": {"value": value, "unit": METRIC, "cores": cpu_threads(),
                              "kind": "port",
-                             "sample": f"{rows} central rows x 1920 px x 64 spp per step"},
+                             "sample": sample.describe(samples // max(1, args.steps),
+                                                       seconds / max(1, args.steps))
+                                       + " (per step)"},
             "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
 
 
+def serve(api, scenes, table, seconds, rng):
+    """Poisson arrivals through the render server; returns latency and throughput figures."""
+    server = api.RenderServer(policy="shortest_first", batch=api.BatchSettings())
+    arrivals = np.cumsum(rng.exponential(1.0 / SERVE_RATE, size=int(SERVE_RATE * seconds * 3)))
+    arrivals = arrivals[arrivals < seconds]
+    picks = rng.integers(0, len(table), size=len(arrivals))
+    # 5% of the jobs are cancelled at a uniform point of their expected life (their samples at
+    # about the plain path's rate) after arrival.
+    events = [(float(at), 0, i) for i, at in enumerate(arrivals)]
+    for i, at in enumerate(arrivals):
+        if rng.random() < CANCEL_FRACTION:
+            job = table[picks[i]]
+            life = job["width"] * job["height"] * job["samples_per_pixel"] / 250e6
+            events.append((float(at + rng.uniform(0, max(life, 1e-3))), 1, i))
+    events.sort()
+    ids = {}
+    t0 = time.perf_counter()
+    for when, kind, i in events:
+        delay = when - (time.perf_counter() - t0)
+        if delay > 0:
+            time.sleep(delay)
+        if kind == 0:
+            job = table[picks[i]]
+            render = api.RenderSettings(job["width"], job["height"], job["samples_per_pixel"],
+                                        job["render_seed"])
+            integrator = api.IntegratorSettings("mis", job["maximum_depth"], True, 3)
+            ids[i] = server.submit(scenes[picks[i]], render, integrator)
+        else:
+            server.cancel(ids[i])
+    latencies, samples, last, first = [], 0, 0.0, None
+    states = {"completed": 0, "cancelled": 0, "failed": 0}
+    for i in range(len(arrivals)):
+        jid = ids[i]
+        server.wait(jid)
+        info = server.info(jid)
+        states[info["state"]] = states.get(info["state"], 0) + 1
+        if info["state"] == "completed":
+            server.result(jid)  # the image in host memory, as a client receives it
+            latencies.append(info["finished"] - info["submitted"])
+            samples += info["total_samples"]
+            last = max(last, info["finished"])
+            first = info["submitted"] if first is None else min(first, info["submitted"])
+        server.release(jid)
+    stats = server.statistics()
+    server.close()
+    span = last - (first or 0.0)
+    return {"arrival_rate_jobs_per_s": SERVE_RATE, "arrival_window_s": seconds,
+            "jobs": len(arrivals), **states,
+            "p50_latency_s": float(np.percentile(latencies, 50)) if latencies else None,
+            "p99_latency_s": float(np.percentile(latencies, 99)) if latencies else None,
+            "samples_per_s_M": samples / span / 1e6 if span > 0 else None,
+            "waves": stats["waves"], "segments": stats["segments"],
+            "latency": "submission to image in host memory (server clock)",
+            "cancellation": "5% of jobs, at a uniform time within their expected duration "
+                            "after arrival"}
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
     from minirender_b200 import _abi, api
+    from minirender_b200 import scene as sc
 
     rank, world, local = rank_info()
     torch.cuda.set_device(local)
@@ -243,100 +344,151 @@ def run_ours(args):
                                 device_id=torch.device("cuda", local))
     lib = _abi.load_library()
 
-    doc = workload()
-    snap = doc.snapshot()
-    seed = rank + 1
-    render = api.RenderSettings(WIDTH, HEIGHT, SPP, seed)
-    integrator = api.IntegratorSettings("mis", DEPTH, True, 3)
-    scene = api.Scene(snap)
-    tracer = api.PathTracer(scene, integrator)
-    stream = torch.cuda.current_stream()
-    image = torch.empty(WIDTH * HEIGHT * 3, dtype=torch.float32, device="cuda")
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
-
-    def frame():
-        flush.fill_(1)
-        tracer.render_device(render, image.data_ptr(), stream.cuda_stream)
-
     def barrier():
         if world > 1:
             dist.barrier()
 
+    table = job_table(args.jobs)
+    for job in table:  # weak scaling: every rank its own render seeds
+        job["render_seed"] += 1000 * rank
+    t0 = time.perf_counter()
+    snaps = [job_document(j).snapshot() for j in table]
+    gen_seconds = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    scenes = [api.Scene(s, split_references=True) for s in snaps]
+    torch.cuda.synchronize()
+    scene_seconds = time.perf_counter() - t0
+    triangles = sum(s.triangle_count for s in snaps)
+    jobs = [api.BatchJob(s, api.RenderSettings(j["width"], j["height"], j["samples_per_pixel"],
+                                               j["render_seed"]),
+                         api.IntegratorSettings("mis", j["maximum_depth"], True, 3))
+            for s, j in zip(scenes, table)]
+    samples = sum(j.render.width * j.render.height * j.render.samples_per_pixel for j in jobs)
+
+    # Autotuner on a calibration subset (every fourth job at 1/16 of its samples), untimed.
+    calib = [api.BatchJob(j.scene, api.RenderSettings(j.render.width, j.render.height,
+                                                      max(1, j.render.samples_per_pixel // 16),
+                                                      j.render.seed), j.integrator)
+             for j in jobs[::4]]
+    t0 = time.perf_counter()
+    tuned, tuned_rate = api.autotune(calib)
+    tune_seconds = time.perf_counter() - t0
+
+    def step():
+        _, codes, info = api.render_batch(jobs, tuned, copy_images=False)
+        assert all(c == 0 for c in codes), codes
+        return info
+
     for _ in range(max(3, args.warmup)):
-        frame()
+        step()
     torch.cuda.synchronize()
 
-    check = lib.mr_set_kernel_timing(1)
-    assert check == 0
     clocks = ClockSampler(local)
     barrier()
     torch.cuda.synchronize()
     clocks.start()
-    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    start.record(stream)
+    device_seconds, wall0 = 0.0, time.perf_counter()
+    launches, waves = 0, 0
     for _ in range(args.steps):
-        frame()
-    stop.record(stream)
+        info = step()
+        device_seconds += info["device_seconds"]
+        launches += info["kernel_launches"]
+        waves += info["waves"]
     torch.cuda.synchronize()
+    wall = time.perf_counter() - wall0
     barrier()
     clock_info = clocks.stop()
-    seconds = start.elapsed_time(stop) / 1e3
-    launches, ksec, all_launches = C.c_uint64(), C.c_double(), C.c_uint64()
-    counted = _abi.TraceStatistics()
-    lib.mr_kernel_timing(C.byref(launches), C.byref(ksec), C.byref(counted), C.byref(all_launches))
-    lib.mr_set_kernel_timing(0)
-    worst = torch.tensor([seconds], dtype=torch.float64, device="cuda")
+    worst = torch.tensor([device_seconds], dtype=torch.float64, device="cuda")
     if world > 1:
         dist.all_reduce(worst, op=dist.ReduceOp.MAX)
     worst = float(worst.item())
-    samples = WIDTH * HEIGHT * SPP
     value = world * samples * args.steps / worst / 1e6
 
-    # Path statistics of one frame (outside the timed region).
-    stats = tracer.render_device(render, image.data_ptr(), stream.cuda_stream, statistics=True)
+    # Plain path on the same jobs: one mr_render_device call per job.
+    stream = torch.cuda.current_stream()
+    image = torch.empty(max(j.render.width * j.render.height for j in jobs) * 3,
+                        dtype=torch.float32, device="cuda")
+    for j in jobs[:4]:
+        api.PathTracer(j.scene, j.integrator).render_device(j.render, image.data_ptr(),
+                                                            stream.cuda_stream)
     torch.cuda.synchronize()
+    assert lib.mr_set_kernel_timing(1) == 0
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for j in jobs:
+        api.PathTracer(j.scene, j.integrator).render_device(j.render, image.data_ptr(),
+                                                            stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    plain_seconds = e0.elapsed_time(e1) / 1e3
+    k_launches, ksec, all_launches = C.c_uint64(), C.c_double(), C.c_uint64()
+    counted = _abi.TraceStatistics()
+    lib.mr_kernel_timing(C.byref(k_launches), C.byref(ksec), C.byref(counted),
+                         C.byref(all_launches))
+    lib.mr_set_kernel_timing(0)
+    plain_value = samples / plain_seconds / 1e6
+
+    # The single 1M-triangle frame (plain path), after one warm-up frame.
+    large = api.Scene(sc.large_scene().snapshot())
+    frame_render = api.RenderSettings(1920, 1080, 64, 1 + rank)
+    frame_tracer = api.PathTracer(large, api.IntegratorSettings("mis", 12, True, 3))
+    frame = torch.empty(1920 * 1080 * 3, dtype=torch.float32, device="cuda")
+    frame_tracer.render_device(frame_render, frame.data_ptr(), stream.cuda_stream)
+    e0.record(stream)
+    frame_tracer.render_device(frame_render, frame.data_ptr(), stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    frame_ms = e0.elapsed_time(e1)
+    large_frame = {"workload": "1920x1080 64 spp depth 12, 1.02M triangles (reference builder)",
+                   "ms": frame_ms, "value": 1920 * 1080 * 64 / frame_ms / 1e3, "unit": METRIC,
+                   "bvh_build_ms": 1e3 * large.build_seconds()}
+    large.close()
 
     # End to end through the public API from pinned host memory.
-    if args.no_e2e:
-        e2e_value, h2d, d2h = None, 0, 0
-        args_e2e = False
-    else:
-        args_e2e = True
-    h2d = pin_snapshot(snap) if args_e2e else 0
-    d2h = WIDTH * HEIGHT * 3 * 4 if args_e2e else 0
+    e2e_value, h2d, d2h = None, 0, 0
+    if not args.no_e2e:
+        h2d = sum(pin_snapshot(s) for s in snaps)
+        d2h = sum(j.render.width * j.render.height * 3 * 4 for j in jobs)
 
-    def e2e_step():
-        s = api.Scene(snap)
-        out, _ = api.PathTracer(s, integrator).render(render, statistics=False)
-        s.close()
-        return out
+        def e2e_step():
+            fresh = [api.Scene(s, split_references=True) for s in snaps]
+            batch = [api.BatchJob(f, j.render, j.integrator) for f, j in zip(fresh, jobs)]
+            _, codes, _ = api.render_batch(batch, tuned)
+            assert all(c == 0 for c in codes), codes
+            for f in fresh:
+                f.close()
 
-    e2e_value = None
-    if args_e2e:
         e2e_step()
         barrier()
         torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
+        w0 = time.perf_counter()
         for _ in range(args.steps):
             e2e_step()
-        e1.record(stream)
         torch.cuda.synchronize()
+        e2e_seconds = torch.tensor([time.perf_counter() - w0], dtype=torch.float64, device="cuda")
         barrier()
-        e2e_seconds = torch.tensor([e0.elapsed_time(e1) / 1e3], dtype=torch.float64, device="cuda")
         if world > 1:
             dist.all_reduce(e2e_seconds, op=dist.ReduceOp.MAX)
         e2e_value = world * samples * args.steps / float(e2e_seconds.item()) / 1e6
+
+    serving = None
+    if world == 1 and not args.no_serve:
+        serving = serve(api, scenes, table, args.serve_seconds, np.random.default_rng(50))
 
     peak, peak_kind = measured_peak()
     algorithmic = (BYTES_PER_BOUNDS_TEST * counted.bounds_tests +
                    BYTES_PER_TRIANGLE_TEST * counted.triangle_tests)
     achieved = algorithmic / ksec.value / 1e9 if ksec.value > 0 else 0.0
+    per_launch = algorithmic / max(1, k_launches.value)
     traffic = None
-    tfile = os.path.join(ROOT, "profiles", "extend_kernel_traffic.txt")
+    tfile = os.path.join(ROOT, "profiles", "trace_kernel_traffic.txt")
     if os.path.exists(tfile):
         with open(tfile) as f:
-            traffic = json.load(f).get("dram_bytes_per_launch")
+            ratio = json.load(f).get("dram_bytes_per_algorithmic_byte")
+        # DRAM bytes per algorithmic byte of the captured launches, applied to this run's
+        # average launch.
+        if ratio:
+            traffic = ratio * per_launch
 
     line = None
     if rank == 0:
@@ -345,30 +497,39 @@ def run_ours(args):
             "steps": args.steps, "warmup": max(3, args.warmup),
             "ms_per_step": 1e3 * worst / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {**config(snap.triangle_count),
-                       "bvh_build_ms": 1e3 * scene.build_seconds(),
-                       "rays_per_frame": {"camera": stats["paths"],
-                                          "extension": stats["scattering_events"],
-                                          "shadow": stats["shadow_rays"]},
-                       "bounds_tests_per_frame": stats["bounds_tests"],
-                       "triangle_tests_per_frame": stats["triangle_tests"]},
-            "roofline": {"bound": "hbm", "kernel": "extend_kernel (nearest-hit traversal)",
+            "config": {**config(table, triangles),
+                       "engine": "batched: mr_render_batch, jobs packed into shared waves",
+                       "autotuned": {"wave_paths": tuned.wave_paths,
+                                     "concurrent_waves": tuned.concurrent_waves,
+                                     "sort_threshold": tuned.sort_threshold,
+                                     "trace_blocks_per_sm": tuned.trace_blocks_per_sm,
+                                     "calibration_Msamples_per_s": tuned_rate / 1e6,
+                                     "tuning_s": tune_seconds},
+                       "wall_ms_per_step": 1e3 * wall / args.steps,
+                       "waves_per_step": waves / args.steps,
+                       "scene_generation_s": gen_seconds, "scene_build_s": scene_seconds,
+                       "plain_gpu": {"value": plain_value, "unit": METRIC,
+                                     "ms_per_step": 1e3 * plain_seconds,
+                                     "engine": "mr_render_device, one job per call"},
+                       "batched_vs_plain": value / plain_value,
+                       "serving": serving, "large_frame": large_frame},
+            "roofline": {"bound": "hbm", "kernel": "trace_kernel (nearest-hit + shadow "
+                                                   "traversal), plain leg of the same jobs",
                          "achieved": achieved, "peak": peak, "peak_source": peak_kind,
-                         "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": traffic,
-                         "algorithmic_bytes_per_launch": algorithmic / max(1, launches.value),
-                         "launches": launches.value,
-                         "avg_launch_ms": 1e3 * ksec.value / max(1, launches.value),
+                         "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                         "algorithmic_bytes_per_launch": per_launch,
+                         "launches": k_launches.value,
+                         "avg_launch_ms": 1e3 * ksec.value / max(1, k_launches.value),
                          "bytes_model": "24 B per bounds test + 36 B per triangle test"},
             "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h,
-                    "step": "scene upload from pinned memory + GPU BVH build + render + "
-                            "image read-back (mr_scene_create + mr_render)"},
-            "gpu_launches": all_launches.value,
+                    "step": "256 scene uploads from pinned memory + GPU BVH builds + batched "
+                            "render + image read-back (mr_scene_create_with + mr_render_batch)"},
+            "gpu_launches": launches,
             "clocks": clock_info,
         }
         if world == 1 and not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline(snap, args.cpu_seconds)
+            line["cpu_baseline"] = cpu_baseline(table, args.cpu_seconds)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

@@ -484,7 +484,9 @@ typedef struct mr_batch_statistics {
     uint64_t           kernel_launches; /* device kernels run (inside graphs or not) */
     uint64_t           graph_launches;
     double             seconds;         /* wall time from the first submission to the last image */
-    double             busy_seconds;    /* device time of the waves */
+    double             busy_seconds;    /* device time of the waves, summed over the lanes */
+    double             device_seconds;  /* CUDA events on the engine's streams: before the first
+                                           wave to after the last resolve */
     mr_path_statistics paths;           /* summed over all jobs */
 } mr_batch_statistics;
 

@@ -167,9 +167,10 @@ class RenderPreview(C.Structure):
                 ("height", C.c_uint64), ("available", C.c_uint32)]
 
 
-# Every exported symbol of include/minirender_b200.h with its ctypes signature.
 P = C.POINTER
 VP = C.c_void_p
+
+
 class BatchSettings(C.Structure):
     _fields_ = [("wave_paths", C.c_uint64), ("trace_blocks_per_sm", C.c_uint32),
                 ("shade_blocks_per_sm", C.c_uint32), ("sort_threshold", C.c_uint32),
@@ -184,7 +185,8 @@ class BatchJob(C.Structure):
 class BatchStatistics(C.Structure):
     _fields_ = [("waves", C.c_uint64), ("segments", C.c_uint64), ("samples", C.c_uint64),
                 ("kernel_launches", C.c_uint64), ("graph_launches", C.c_uint64),
-                ("seconds", C.c_double), ("busy_seconds", C.c_double), ("paths", PathStatistics)]
+                ("seconds", C.c_double), ("busy_seconds", C.c_double),
+                ("device_seconds", C.c_double), ("paths", PathStatistics)]
 
 
 class ServerSettings(C.Structure):
@@ -206,6 +208,7 @@ class ServerStatistics(C.Structure):
                [("busy_seconds", C.c_double), ("elapsed_seconds", C.c_double)]
 
 
+# Every exported symbol of include/minirender_b200.h with its ctypes signature.
 SIGNATURES = {
     "mr_abi_version": (C.c_uint32, []),
     "mr_last_error": (C.c_size_t, [C.c_char_p, C.c_size_t]),

@@ -382,11 +382,14 @@ def _batch_records(jobs, images):
     return records
 
 
-def render_batch(jobs: list[BatchJob], settings: BatchSettings | None = None):
+def render_batch(jobs: list[BatchJob], settings: BatchSettings | None = None,
+                 copy_images: bool = True):
     """Renders many jobs together (mr_render_batch). Returns the images ((H, W, 3) float32, None
-    for a job that failed), the per-job status codes and the batch statistics."""
+    for a job that failed or when `copy_images` is false: the images then stay on the device
+    and are dropped), the per-job status codes and the batch statistics."""
     lib = load_library()
-    images = [np.zeros((j.render.height, j.render.width, 3), np.float32) for j in jobs]
+    images = ([np.zeros((j.render.height, j.render.width, 3), np.float32) for j in jobs]
+              if copy_images else None)
     records = _batch_records(jobs, images)
     stats = _abi.BatchStatistics()
     bs = (settings or BatchSettings()).c()
@@ -394,9 +397,11 @@ def render_batch(jobs: list[BatchJob], settings: BatchSettings | None = None):
     codes = [records[i].status for i in range(len(jobs))]
     if status != _abi.MR_OK and all(c == _abi.MR_OK for c in codes):
         check(status, lib)
-    out = [img if code == _abi.MR_OK else None for img, code in zip(images, codes)]
+    out = ([img if code == _abi.MR_OK else None for img, code in zip(images, codes)]
+           if copy_images else [None] * len(jobs))
     info = {k: getattr(stats, k) for k in ("waves", "segments", "samples", "kernel_launches",
-                                           "graph_launches", "seconds", "busy_seconds")}
+                                           "graph_launches", "seconds", "busy_seconds",
+                                           "device_seconds")}
     info["paths"] = stats.paths.as_dict()
     return out, codes, info
 

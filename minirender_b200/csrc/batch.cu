@@ -447,6 +447,15 @@ class Server {
         return s;
     }
 
+    // Records `e` on the admin stream behind everything enqueued on the lanes so far (device
+    // timestamps around a batch).
+    void record_after_lanes(cudaEvent_t e) {
+        std::lock_guard<std::mutex> lock(mutex_);
+        DeviceGuard                 guard(device_);
+        admin_after_lanes();
+        MR_CUDA(cudaEventRecord(e, stream_));
+    }
+
     // Path statistics summed over every wave so far (waits for the waves in flight).
     mr_path_statistics path_statistics() {
         cudaEvent_t e = nullptr;
@@ -929,6 +938,10 @@ mr_status run_batch(mr_batch_job* jobs, size_t count, const mr_batch_settings* s
     }
     const auto t0 = Clock::now();
     Server     server(ss);
+    cudaEvent_t marks[2] = {nullptr, nullptr};
+    MR_CUDA(cudaEventCreate(&marks[0]));
+    MR_CUDA(cudaEventCreate(&marks[1]));
+    server.record_after_lanes(marks[0]);
     std::vector<uint64_t> ids(count, 0);
     mr_status first = MR_OK;
     for (size_t i = 0; i < count; ++i) {
@@ -945,6 +958,12 @@ mr_status run_batch(mr_batch_job* jobs, size_t count, const mr_batch_settings* s
     }
     server.wait_all();
     const double seconds = std::chrono::duration<double>(Clock::now() - t0).count();
+    server.record_after_lanes(marks[1]);
+    float device_ms = 0;
+    MR_CUDA(cudaEventSynchronize(marks[1]));
+    MR_CUDA(cudaEventElapsedTime(&device_ms, marks[0], marks[1]));
+    cudaEventDestroy(marks[0]);
+    cudaEventDestroy(marks[1]);
     for (size_t i = 0; i < count; ++i) {
         if (ids[i] == 0) {
             continue;
@@ -968,6 +987,7 @@ mr_status run_batch(mr_batch_job* jobs, size_t count, const mr_batch_settings* s
         statistics->graph_launches  = s.graph_launches;
         statistics->seconds         = seconds;
         statistics->busy_seconds    = s.busy_seconds;
+        statistics->device_seconds  = device_ms * 1e-3;
         statistics->paths           = server.path_statistics();
     }
     return first;
