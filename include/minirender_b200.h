@@ -394,11 +394,21 @@ mr_status mr_render(const mr_scene* scene, const mr_integrator_settings* integra
                     const mr_render_settings* render, float* rgb, mr_path_statistics* statistics);
 
 /* PathTracer::render with the image left in device memory: `device_rgb` is a device pointer
- * to width*height*3 floats and `stream` a cudaStream_t (null = the legacy default stream).
- * The call is asynchronous with respect to the host unless `statistics` is non-null. */
+ * to width*height*3 floats and `stream` a cudaStream_t (null = the legacy default stream). The
+ * work runs on `stream`; the call returns once it has finished (it reads the frame's error
+ * words and statistics back). */
 mr_status mr_render_device(const mr_scene* scene, const mr_integrator_settings* integrator,
                            const mr_render_settings* render, float* device_rgb, void* stream,
                            mr_path_statistics* statistics);
+
+/* Rows [row_begin, row_end) of PathTracer::render's image into `rgb` (width*(row_end-row_begin)*3
+ * host floats). Every pixel equals the full render's pixel bit for bit (each pixel's samples are
+ * its own streams, summed in sample order), so ranks can render row bands of one frame and
+ * gather them. No reference counterpart: the reference's tile loop is internal to
+ * RenderSession (src/render/render_session.cpp:363-459). Statistics cover the band. */
+mr_status mr_render_rows(const mr_scene* scene, const mr_integrator_settings* integrator,
+                         const mr_render_settings* render, uint64_t row_begin, uint64_t row_end,
+                         float* rgb, mr_path_statistics* statistics);
 
 /* display_image (src/render/path_tracer.cpp:540-557): exposure + Reinhard on a host image. */
 mr_status mr_display_image(const float* linear, uint64_t width, uint64_t height, double exposure,

@@ -233,6 +233,8 @@ SIGNATURES = {
     "mr_trace_paths_static": (C.c_int, [VP, P(IntegratorSettings), VP, VP, C.c_size_t, VP, VP]),
     "mr_render": (C.c_int, [VP, P(IntegratorSettings), P(RenderSettings), P(C.c_float),
                             P(PathStatistics)]),
+    "mr_render_rows": (C.c_int, [VP, P(IntegratorSettings), P(RenderSettings), C.c_uint64,
+                                 C.c_uint64, P(C.c_float), P(PathStatistics)]),
     "mr_render_device": (C.c_int, [VP, P(IntegratorSettings), P(RenderSettings), VP, VP,
                                    P(PathStatistics)]),
     "mr_display_image": (C.c_int, [P(C.c_float), C.c_uint64, C.c_uint64, C.c_double,

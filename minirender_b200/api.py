@@ -233,6 +233,19 @@ class PathTracer:
               self.lib)
         return out, stats.as_dict()
 
+    def render_rows(self, render: RenderSettings, row_begin: int, row_end: int,
+                    statistics: bool = False):
+        """Rows [row_begin, row_end) of render(): ((row_end-row_begin), width, 3) float32, bit
+        for bit the full image's rows."""
+        out = np.zeros((max(0, row_end - row_begin), render.width, 3), np.float32)
+        stats = _abi.PathStatistics()
+        settings, rs = self.settings.c(), render.c()
+        check(self.lib.mr_render_rows(self.scene.handle, C.byref(settings), C.byref(rs),
+                                      row_begin, row_end,
+                                      _ptr(out, C.c_float) if out.size else None,
+                                      C.byref(stats) if statistics else None), self.lib)
+        return (out, stats.as_dict()) if statistics else out
+
     def render_device(self, render: RenderSettings, device_ptr: int, stream: int = 0,
                       statistics: bool = False):
         """PathTracer::render into device memory (a pointer from the caller's allocator)."""

@@ -649,6 +649,31 @@ mr_status mr_render_device(const mr_scene* scene, const mr_integrator_settings* 
     });
 }
 
+mr_status mr_render_rows(const mr_scene* scene, const mr_integrator_settings* integrator,
+                         const mr_render_settings* render, uint64_t row_begin, uint64_t row_end,
+                         float* rgb, mr_path_statistics* statistics) {
+    return guarded([&] {
+        const Scene&           s = scene_of(scene);
+        const IntegratorParams p = integrator_params(integrator);
+        validate_render(render);
+        require(row_begin <= row_end && row_end <= render->height, "Row range is outside the image");
+        require(rgb != nullptr || row_begin == row_end, "Output image is null");
+        const size_t pixels = static_cast<size_t>(render->width) * (row_end - row_begin);
+        mr_path_statistics local{};
+        if (pixels == 0) {
+            if (statistics) {
+                *statistics = local;
+            }
+            return;
+        }
+        DeviceBuffer<float> image;
+        image.allocate(3 * pixels);
+        render_frame(s, p, *render, image.ptr, nullptr, statistics ? statistics : &local, 0,
+                     static_cast<uint32_t>(row_begin), static_cast<uint32_t>(row_end));
+        MR_CUDA(cudaMemcpy(rgb, image.ptr, 3 * pixels * sizeof(float), cudaMemcpyDeviceToHost));
+    });
+}
+
 mr_status mr_render(const mr_scene* scene, const mr_integrator_settings* integrator,
                     const mr_render_settings* render, float* rgb, mr_path_statistics* statistics) {
     return guarded([&] {

@@ -619,14 +619,14 @@ __device__ __forceinline__ void neumaier(float& sum, float& comp, float v) {
 // like check_radiance (src/render/path_tracer.cpp:155-159).
 __global__ void resolve_kernel(const float4* radiance, uint32_t x0, uint32_t y0, uint32_t w,
                                uint32_t h, uint32_t ns, uint32_t width, float4* accumulator,
-                               unsigned* error) {
+                               uint32_t accumulator_row0, unsigned* error) {
     const uint32_t r    = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t area = w * h;
     if (r >= area) {
         return;
     }
     const uint32_t ry    = r / w;
-    const size_t   pixel = static_cast<size_t>(y0 + ry) * width + x0 + (r - ry * w);
+    const size_t   pixel = static_cast<size_t>(y0 + ry - accumulator_row0) * width + x0 + (r - ry * w);
     float4         sum   = accumulator[2 * pixel];
     float4         comp  = accumulator[2 * pixel + 1];
     bool           bad   = false;
@@ -1069,7 +1069,7 @@ void Engine::enqueue_batch_resolve(const WaveDesc* wave, Workspace& ws, cudaStre
 
 void render_tile(const Scene& scene, const IntegratorParams& params, const mr_render_settings& render,
                  uint32_t x0, uint32_t y0, uint32_t w, uint32_t h, uint32_t s0, uint32_t ns,
-                 float4* accumulator, Workspace& ws, cudaStream_t stream) {
+                 float4* accumulator, Workspace& ws, cudaStream_t stream, uint32_t accumulator_row0) {
     const size_t area = static_cast<size_t>(w) * h;
     if (area == 0 || ns == 0) {
         return;
@@ -1098,7 +1098,7 @@ void render_tile(const Scene& scene, const IntegratorParams& params, const mr_re
             note_launches(1);
             resolve_kernel<<<static_cast<unsigned>((a + 255) / 256), 256, 0, stream>>>(
                 ws.state.radiance, init.x0, init.y0, w, hh, init.ns, init.width, accumulator,
-                ws.queues.error);
+                accumulator_row0, ws.queues.error);
         }
     }
     MR_CUDA(cudaGetLastError());
@@ -1106,16 +1106,23 @@ void render_tile(const Scene& scene, const IntegratorParams& params, const mr_re
 
 void render_frame(const Scene& scene, const IntegratorParams& params, const mr_render_settings& render,
                   float* device_rgb, cudaStream_t stream, mr_path_statistics* statistics,
-                  size_t max_paths) {
-    const size_t pixels   = static_cast<size_t>(render.width) * render.height;
+                  size_t max_paths, uint32_t row_begin, uint32_t row_end) {
+    row_end               = std::min<uint32_t>(row_end, static_cast<uint32_t>(render.height));
+    const uint32_t rows   = row_end > row_begin ? row_end - row_begin : 0;
+    const size_t pixels   = static_cast<size_t>(render.width) * rows;
     const size_t total    = pixels * render.samples_per_pixel;
+    if (total == 0) {
+        if (statistics) {
+            *statistics = {};
+        }
+        return;
+    }
     const size_t capacity = std::min(total, max_paths ? max_paths : (size_t(1) << 23));
     auto         ws       = acquire_workspace(capacity, params.maximum_depth + 1, pixels);
     reset_statistics(*ws, stream);
     MR_CUDA(cudaMemsetAsync(ws->accumulator, 0, 2 * pixels * sizeof(float4), stream));
-    render_tile(scene, params, render, 0, 0, static_cast<uint32_t>(render.width),
-                static_cast<uint32_t>(render.height), 0, render.samples_per_pixel, ws->accumulator,
-                *ws, stream);
+    render_tile(scene, params, render, 0, row_begin, static_cast<uint32_t>(render.width), rows, 0,
+                render.samples_per_pixel, ws->accumulator, *ws, stream, row_begin);
     note_launches(1);
     finalize_kernel<<<static_cast<unsigned>((pixels + 255) / 256), 256, 0, stream>>>(
         ws->accumulator, pixels, render.samples_per_pixel, device_rgb, ws->queues.error);

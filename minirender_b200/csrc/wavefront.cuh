@@ -202,15 +202,18 @@ inline void note_launches(uint64_t n) {
 
 // Frame render into a device image (width*height*3 floats) — used by mr_render(_device) and the
 // session. Statistics (optional) are read back after the frame.
+// With row_begin/row_end the rows [row_begin, row_end) of the frame are rendered into a
+// width*(row_end-row_begin)*3 image; every pixel is the full frame's pixel bit for bit.
 void render_frame(const Scene& scene, const IntegratorParams& params, const mr_render_settings& render,
                   float* device_rgb, cudaStream_t stream, mr_path_statistics* statistics,
-                  size_t max_paths = 0);
+                  size_t max_paths = 0, uint32_t row_begin = 0, uint32_t row_end = 0xFFFFFFFFu);
 
 // Accumulates the samples [s0, s0+ns) of a pixel rectangle into a caller-owned Kahan
 // accumulator (float4 sum + float4 compensation per pixel of the full image).
+// The accumulator's first row is image row `accumulator_row0`.
 void render_tile(const Scene& scene, const IntegratorParams& params, const mr_render_settings& render,
                  uint32_t x0, uint32_t y0, uint32_t w, uint32_t h, uint32_t s0, uint32_t ns,
-                 float4* accumulator, Workspace& ws, cudaStream_t stream);
+                 float4* accumulator, Workspace& ws, cudaStream_t stream, uint32_t accumulator_row0 = 0);
 
 void read_statistics(Workspace& ws, cudaStream_t stream, mr_path_statistics* out, unsigned* error);
 void reset_statistics(Workspace& ws, cudaStream_t stream);

@@ -166,3 +166,19 @@ def test_autotune_returns_a_valid_shape(api, scenes):
     images, codes, _ = api.render_batch(jobs, best)
     assert codes == [0, 0]
     np.testing.assert_array_equal(images[0], plain(api, jobs[0]))
+
+
+def test_row_bands_assemble_the_frame_bitwise(api, scenes):
+    from minirender_b200 import shard
+    render = api.RenderSettings(83, 61, 6, 12)
+    for scene in scenes[:2]:
+        tracer = api.PathTracer(scene, api.IntegratorSettings("mis", 9, True, 3))
+        full, stats = tracer.render(render)
+        bands = [tracer.render_rows(render, b, e) for b, e in shard.row_bands(render.height, 3)]
+        np.testing.assert_array_equal(np.concatenate(bands), full)
+        rows, band_stats = tracer.render_rows(render, 0, render.height, statistics=True)
+        np.testing.assert_array_equal(rows, full)
+        assert band_stats["paths"] == stats["paths"]
+    assert tracer.render_rows(render, 5, 5).shape == (0, 83, 3)
+    with pytest.raises(api.MiniRenderError):
+        tracer.render_rows(render, 10, 62)
