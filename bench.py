@@ -71,9 +71,42 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-serve", action="store_true")
-    # Profiling aid (ncu captures): render only the first J jobs. The default is the benchmark.
-    p.add_argument("--jobs", type=int, default=JOBS)
+    # Profiling aids (ncu captures); the defaults are the benchmark.
+    p.add_argument("--jobs", type=int, default=JOBS, help="render only the first J jobs")
+    p.add_argument("--no-autotune", action="store_true", help="default wave shape, no tuning")
+    p.add_argument("--trace-sample", type=int, default=None, metavar="K",
+                   help="render job K once on the plain path with kernel timing, print the "
+                        "traversal work of its trace launches, and exit")
     return p.parse_args()
+
+
+def trace_sample(k):
+    """One plain render of job K with the traversal kernels' work counted: the algorithmic
+    bytes an ncu capture of the same command divides its DRAM bytes by."""
+    import torch
+    from minirender_b200 import _abi, api
+    job = job_table(JOBS)[k]
+    scene = api.Scene(job_document(job).snapshot(), split_references=True)
+    render = api.RenderSettings(job["width"], job["height"], job["samples_per_pixel"],
+                                job["render_seed"])
+    tracer = api.PathTracer(scene, api.IntegratorSettings("mis", job["maximum_depth"], True, 3))
+    image = torch.empty(job["width"] * job["height"] * 3, dtype=torch.float32, device="cuda")
+    lib = _abi.load_library()
+    assert lib.mr_set_kernel_timing(1) == 0
+    tracer.render_device(render, image.data_ptr())
+    torch.cuda.synchronize()
+    launches, seconds, all_launches = C.c_uint64(), C.c_double(), C.c_uint64()
+    counted = _abi.TraceStatistics()
+    lib.mr_kernel_timing(C.byref(launches), C.byref(seconds), C.byref(counted), C.byref(all_launches))
+    lib.mr_set_kernel_timing(0)
+    algorithmic = (BYTES_PER_BOUNDS_TEST * counted.bounds_tests +
+                   BYTES_PER_TRIANGLE_TEST * counted.triangle_tests)
+    print(json.dumps({"job": k, **job, "trace_launches": launches.value,
+                      "bounds_tests": counted.bounds_tests,
+                      "triangle_tests": counted.triangle_tests,
+                      "algorithmic_bytes": algorithmic, "trace_seconds": seconds.value,
+                      "all_launches": all_launches.value}), flush=True)
+    return 0
 
 
 def rank_info():
@@ -371,7 +404,10 @@ def run_ours(args):
                                                       j.render.seed), j.integrator)
              for j in jobs[::4]]
     t0 = time.perf_counter()
-    tuned, tuned_rate = api.autotune(calib)
+    if args.no_autotune:
+        tuned, tuned_rate = api.BatchSettings(), 0.0
+    else:
+        tuned, tuned_rate = api.autotune(calib)
     tune_seconds = time.perf_counter() - t0
 
     def step():
@@ -540,6 +576,8 @@ def run_ours(args):
 
 def main():
     args = parse()
+    if args.trace_sample is not None:
+        return trace_sample(args.trace_sample)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)
