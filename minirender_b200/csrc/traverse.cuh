@@ -158,6 +158,9 @@ struct TraceCounters {
 };
 
 // Nearest hit (ANY_HIT = false) or occlusion (ANY_HIT = true) in [tmin, tmax].
+// Lanes of a warp traverse interior nodes together and postpone the first leaf they reach until
+// every active lane holds one (or has finished), then test leaves together: interior and leaf
+// work are not interleaved across lanes.
 template <bool ANY_HIT>
 __device__ __forceinline__ TraceResult trace(const DeviceScene& s, const RayQuery& q, float tmin,
                                              float tmax, TraceCounters& counters,
@@ -173,7 +176,6 @@ __device__ __forceinline__ TraceResult trace(const DeviceScene& s, const RayQuer
         error |= kErrorRay;
         return result;
     }
-    // The root's own box (src/render/bvh.cpp:331-334).
     counters.bounds++;
     const float root_enter =
         slab_enter(q, make_float4(s.root_lo[0], s.root_hi[0], s.root_lo[1], s.root_hi[1]),
@@ -181,26 +183,45 @@ __device__ __forceinline__ TraceResult trace(const DeviceScene& s, const RayQuer
     if (!(root_enter <= tmax)) {
         return result;
     }
-    int2  stack[kStackSize];
-    int   sp        = 0;
-    int      node      = s.root;
-    float    node_tmin = root_enter;
-    uint32_t visits    = 0;
-    while (true) {
-        if (++visits > kMaxVisits) {  // only a malformed tree can get here
-            error |= kErrorVisits;
-            return result;
+    int2     stack[kStackSize];
+    int      sp     = 0;
+    int      node   = s.root;  // next node to visit (interior >= 0, leaf < 0)
+    bool     alive  = true;    // `node` is valid
+    int      leaf   = 0;
+    bool     held   = false;   // a postponed leaf in `leaf`
+    uint32_t visits = 0;
+    const float inf = __int_as_float(0x7f800000);
+    // Next stacked subtree that can still contain a nearer hit, or none.
+    const auto pop = [&]() {
+        while (sp > 0) {
+            const int2 e = stack[--sp];
+            if (__int_as_float(e.y) <= result.t) {
+                node = e.x;
+                return;
+            }
         }
-        if (node >= 0) {
-            // Wide node: four slab tests, children visited near to far (the reference's
-            // near-first order generalised; results do not depend on the order).
+        alive = false;
+    };
+    // Every pass of every loop below visits a node or tests a leaf, and both count against
+    // kMaxVisits, so traversal ends on any input.
+    while (alive || held) {
+        if (alive && node < 0 && !held) {  // a leaf to test next (also a root that is a leaf)
+            leaf = node;
+            held = true;
+            pop();
+        }
+        // Interior phase.
+        while (alive && node >= 0) {
+            if (++visits > kMaxVisits) {
+                error |= kErrorVisits;
+                return result;
+            }
             const float4* n   = s.nodes + 8 * static_cast<size_t>(node);
             const float4  lox = __ldg(n + 0), hix = __ldg(n + 1);
             const float4  loy = __ldg(n + 2), hiy = __ldg(n + 3);
             const float4  loz = __ldg(n + 4), hiz = __ldg(n + 5);
             const int4    ref = __ldg(reinterpret_cast<const int4*>(n + 6));
             counters.bounds += static_cast<uint32_t>(__ldg(reinterpret_cast<const int*>(n + 7)));
-            const float inf = __int_as_float(0x7f800000);
             float t0 = slab_enter6(q, lox.x, hix.x, loy.x, hiy.x, loz.x, hiz.x, tmin, result.t);
             float t1 = slab_enter6(q, lox.y, hix.y, loy.y, hiy.y, loz.y, hiz.y, tmin, result.t);
             float t2 = slab_enter6(q, lox.z, hix.z, loy.z, hiy.z, loz.z, hiz.z, tmin, result.t);
@@ -230,13 +251,26 @@ __device__ __forceinline__ TraceResult trace(const DeviceScene& s, const RayQuer
                 if (t1 != inf) {
                     stack[sp++] = make_int2(r1, __float_as_int(t1));
                 }
-                node      = r0;
-                node_tmin = t0;
-                continue;
+                node = r0;
+            } else {
+                pop();
             }
-        } else {
-            // Leaf: triangles from slot ~node until the leaf-end flag.
-            for (uint32_t slot = static_cast<uint32_t>(~node);; ++slot) {
+            if (alive && node < 0 && !held) {  // postpone the first leaf and keep descending
+                leaf = node;
+                held = true;
+                pop();
+            }
+            if (!__any_sync(__activemask(), !held)) {
+                break;  // every lane here holds a leaf
+            }
+        }
+        // Leaf phase: the postponed leaf, then any leaf the lane now points at.
+        while (held) {
+            if (++visits > kMaxVisits) {
+                error |= kErrorVisits;
+                return result;
+            }
+            for (uint32_t slot = static_cast<uint32_t>(~leaf);; ++slot) {
                 const float4* tp = s.tris + 3 * static_cast<size_t>(slot);
                 const float4  a4 = __ldg(tp + 0);
                 const float4  b4 = __ldg(tp + 1);
@@ -248,7 +282,6 @@ __device__ __forceinline__ TraceResult trace(const DeviceScene& s, const RayQuer
                                   det)) {
                     bool visible = true;
                     if (flags & kTriSingleSided) {
-                        // Outward normal from the winding (src/render/bvh.cpp:369-381).
                         const f3 outward = cross(xyz(b4) - xyz(a4), xyz(c4) - xyz(a4));
                         const float side = dot(q.d, outward);
                         visible = (flags & kTriMirrored) ? side > 0 : side < 0;
@@ -272,20 +305,15 @@ __device__ __forceinline__ TraceResult trace(const DeviceScene& s, const RayQuer
                     break;
                 }
             }
-        }
-        // Pop the next subtree that can still contain a nearer hit.
-        while (true) {
-            if (sp == 0) {
-                return result;
-            }
-            const int2 e = stack[--sp];
-            node_tmin    = __int_as_float(e.y);
-            node         = e.x;
-            if (node_tmin <= result.t) {
-                break;
+            held = false;
+            if (alive && node < 0) {
+                leaf = node;
+                held = true;
+                pop();
             }
         }
     }
+    return result;
 }
 
 }  // namespace mr

@@ -105,9 +105,19 @@ def test_server_pause_resume_cancel(api, scenes):
         server.cancel(victim)
         assert server.info(victim)["state"] == "cancelled"
         assert server.wait(small, 60_000)
+        # Pause acts at the next wave: waves already enqueued with the job still retire. Once
+        # they have, the job makes no progress while paused.
+        deadline = time.time() + 30
         held = server.info(big)["completed_samples"]
-        time.sleep(0.2)
-        assert server.info(big)["completed_samples"] == held  # no progress while paused
+        while True:
+            time.sleep(0.2)
+            now = server.info(big)["completed_samples"]
+            if now == held:
+                break
+            held = now
+            assert time.time() < deadline
+        time.sleep(0.3)
+        assert server.info(big)["completed_samples"] == held < 128 * 128 * 64
         preview, passes = server.preview(big)
         assert np.isfinite(preview).all() and passes < 64
         assert server.resume(big)
