@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <numeric>
 
 #include "errors.hpp"
@@ -373,6 +374,29 @@ void validate_imported(const mr_bvh_desc& b, uint32_t prims) {
 
 }  // namespace
 
+cudaMemPool_t library_pool() {
+    static std::mutex                  mutex;
+    static std::vector<cudaMemPool_t> pools;
+    int device = 0;
+    MR_CUDA(cudaGetDevice(&device));
+    std::lock_guard<std::mutex> lock(mutex);
+    if (pools.size() <= static_cast<size_t>(device)) {
+        pools.resize(device + 1, nullptr);
+    }
+    if (!pools[device]) {
+        cudaMemPoolProps props{};
+        props.allocType     = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id   = device;
+        cudaMemPool_t pool  = nullptr;
+        MR_CUDA(cudaMemPoolCreate(&pool, &props));
+        uint64_t keep = 2ull << 30;
+        MR_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+        pools[device] = pool;
+    }
+    return pools[device];
+}
+
 std::unique_ptr<Scene> create_scene(const mr_scene_desc& desc, const mr_bvh_desc* bvh,
                                     const mr_build_settings* build) {
     int device_count = 0;
@@ -451,8 +475,15 @@ std::unique_ptr<Scene> create_scene(const mr_scene_desc& desc, const mr_bvh_desc
         validate_imported(*bvh, prims);
     }
 
-    cudaStream_t stream = nullptr;
-    size_t       bytes  = 0;
+    // Construction runs on its own stream with stream-ordered buffers (see AllocationScope).
+    struct OwnedStream {
+        cudaStream_t stream = nullptr;
+        OwnedStream() { MR_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking)); }
+        ~OwnedStream() { cudaStreamDestroy(stream); }
+    } owned;
+    cudaStream_t    stream = owned.stream;
+    AllocationScope scope(stream);
+    size_t          bytes = 0;
 
     // ---- upload meshes and instances ----
     DeviceBuffer<float>          positions;

@@ -10,28 +10,67 @@
 
 namespace mr {
 
-// Owning device allocation (cudaMalloc/cudaFree), movable only.
+// The library's stream-ordered device memory pool of the current device (created on first use;
+// keeps up to 2 GB of freed memory for reuse).
+cudaMemPool_t library_pool();
+
+// While an AllocationScope is alive on a thread, DeviceBuffers allocated on that thread come from
+// the library pool, ordered on the scope's stream, and those released inside the same scope are
+// freed ordered on it too: no device-wide synchronisation, so scene construction can run beside
+// rendering and beside other constructions. Buffers that outlive the scope are freed with
+// cudaFree later. Outside any scope DeviceBuffer uses cudaMalloc/cudaFree.
+struct AllocationScope {
+    static inline thread_local cudaStream_t current    = nullptr;
+    static inline thread_local uint64_t     current_id = 0;
+    static inline thread_local uint64_t     next_id    = 0;
+    cudaStream_t previous;
+    uint64_t     previous_id;
+    explicit AllocationScope(cudaStream_t stream) : previous(current), previous_id(current_id) {
+        current    = stream;
+        current_id = ++next_id;
+    }
+    ~AllocationScope() {
+        current    = previous;
+        current_id = previous_id;
+    }
+    AllocationScope(const AllocationScope&)            = delete;
+    AllocationScope& operator=(const AllocationScope&) = delete;
+};
+
+// Owning device allocation, movable only.
 template <typename T> struct DeviceBuffer {
-    T*     ptr   = nullptr;
-    size_t count = 0;
+    T*       ptr   = nullptr;
+    size_t   count = 0;
+    uint64_t scope = 0;  // AllocationScope id of a pooled allocation, 0 for cudaMalloc
     DeviceBuffer() = default;
     DeviceBuffer(const DeviceBuffer&) = delete;
     DeviceBuffer& operator=(const DeviceBuffer&) = delete;
-    DeviceBuffer(DeviceBuffer&& o) noexcept : ptr(o.ptr), count(o.count) { o.ptr = nullptr; o.count = 0; }
+    DeviceBuffer(DeviceBuffer&& o) noexcept : ptr(o.ptr), count(o.count), scope(o.scope) {
+        o.ptr   = nullptr;
+        o.count = 0;
+        o.scope = 0;
+    }
     DeviceBuffer& operator=(DeviceBuffer&& o) noexcept {
         release();
-        ptr = o.ptr;
-        count = o.count;
-        o.ptr = nullptr;
+        ptr     = o.ptr;
+        count   = o.count;
+        scope   = o.scope;
+        o.ptr   = nullptr;
         o.count = 0;
+        o.scope = 0;
         return *this;
     }
     ~DeviceBuffer() { release(); }
     void release() {
         if (ptr) {
-            cudaFree(ptr);
+            if (scope != 0 && scope == AllocationScope::current_id) {
+                cudaFreeAsync(ptr, AllocationScope::current);
+            } else {
+                cudaFree(ptr);
+            }
             ptr   = nullptr;
             count = 0;
+            scope = 0;
         }
     }
     void allocate(size_t n) {  // throws Error (MR_OUT_OF_MEMORY / MR_CUDA_ERROR)
@@ -39,7 +78,13 @@ template <typename T> struct DeviceBuffer {
         if (n == 0) {
             return;
         }
-        MR_CUDA(cudaMalloc(reinterpret_cast<void**>(&ptr), n * sizeof(T)));
+        if (AllocationScope::current_id != 0) {
+            MR_CUDA(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&ptr), n * sizeof(T), library_pool(),
+                                            AllocationScope::current));
+            scope = AllocationScope::current_id;
+        } else {
+            MR_CUDA(cudaMalloc(reinterpret_cast<void**>(&ptr), n * sizeof(T)));
+        }
         count = n;
     }
     size_t bytes() const { return count * sizeof(T); }
