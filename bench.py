@@ -19,7 +19,8 @@ inputs (scenes: tens of millions of triangles; path state: GBs) exceed L2, so no
 Beside it, on the same jobs and scenes: the plain one-job-per-call path (mr_render_device per job,
 CUDA events on the caller's stream, kernel timing of the traversal kernel for the roofline), a
 serving run (Poisson arrivals at 50 jobs/s through the render server, 5% cancelled, p50/p99
-latency from submission to image in host memory), and the single 1M-triangle frame
+latency from submission to image in host memory; again at 16 jobs/s, a load one B200 keeps up
+with), and the single 1M-triangle frame
 (1920x1080, 64 spp, depth 12). `e2e` repeats the step through the public API from pinned host
 memory: every step creates the 256 scenes (upload + GPU build, on 8 host threads) and renders
 them with images read back to host memory. Multi-GPU runs are weak-scaled: each rank renders its own copy of the job
@@ -54,7 +55,8 @@ FALLBACK_HBM_GBS = 6650.0
 BYTES_PER_BOUNDS_TEST = 24   # one FP32 AABB
 BYTES_PER_TRIANGLE_TEST = 36  # one FP32 triangle
 CPU_SAMPLE_JOBS = (0, 64, 128, 192)
-SERVE_RATE = 50.0             # jobs per second
+SERVE_RATE = 50.0             # jobs per second (the serving workload)
+SUSTAINABLE_RATE = 16.0       # jobs per second that one B200 keeps up with on this job mix
 CANCEL_FRACTION = 0.05
 
 
@@ -71,6 +73,9 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-serve", action="store_true")
+    p.add_argument("--stress", action="store_true",
+                   help="also render the 20M-triangle scene in a medium at 3840x2160, 256 spp, "
+                        "depth 16 (about half a minute)")
     # Profiling aids (ncu captures); the defaults are the benchmark.
     p.add_argument("--jobs", type=int, default=JOBS, help="render only the first J jobs")
     p.add_argument("--no-autotune", action="store_true", help="default wave shape, no tuning")
@@ -306,10 +311,10 @@ def run_reference(args):
     return 0
 
 
-def serve(api, scenes, table, seconds, rng):
+def serve(api, scenes, table, seconds, rng, rate=SERVE_RATE):
     """Poisson arrivals through the render server; returns latency and throughput figures."""
     server = api.RenderServer(policy="shortest_first", batch=api.BatchSettings())
-    arrivals = np.cumsum(rng.exponential(1.0 / SERVE_RATE, size=int(SERVE_RATE * seconds * 3)))
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=int(rate * seconds * 3) + 8))
     arrivals = arrivals[arrivals < seconds]
     picks = rng.integers(0, len(table), size=len(arrivals))
     # 5% of the jobs are cancelled at a uniform point of their expected life (their samples at
@@ -352,7 +357,7 @@ def serve(api, scenes, table, seconds, rng):
     stats = server.statistics()
     server.close()
     span = last - (first or 0.0)
-    return {"arrival_rate_jobs_per_s": SERVE_RATE, "arrival_window_s": seconds,
+    return {"arrival_rate_jobs_per_s": rate, "arrival_window_s": seconds,
             "jobs": len(arrivals), **states,
             "p50_latency_s": float(np.percentile(latencies, 50)) if latencies else None,
             "p99_latency_s": float(np.percentile(latencies, 99)) if latencies else None,
@@ -512,9 +517,33 @@ def run_ours(args):
             dist.all_reduce(e2e_seconds, op=dist.ReduceOp.MAX)
         e2e_value = world * samples * args.steps / float(e2e_seconds.item()) / 1e6
 
-    serving = None
+    serving = sustainable = None
     if world == 1 and not args.no_serve:
         serving = serve(api, scenes, table, args.serve_seconds, np.random.default_rng(50))
+        sustainable = serve(api, scenes, table, args.serve_seconds, np.random.default_rng(16),
+                            SUSTAINABLE_RATE)
+
+    stress = None
+    if args.stress:
+        doc = sc.stress_scene()
+        t0 = time.perf_counter()
+        big = api.Scene(doc.snapshot())
+        torch.cuda.synchronize()
+        build_s = time.perf_counter() - t0
+        tracer = api.PathTracer(big, api.IntegratorSettings("mis", 16, True, 3))
+        out = torch.empty(3840 * 2160 * 3, dtype=torch.float32, device="cuda")
+        tracer.render_device(api.RenderSettings(960, 540, 4, 1), out.data_ptr(), stream.cuda_stream)
+        full = api.RenderSettings(3840, 2160, 256, 1 + rank)
+        e0.record(stream)
+        tracer.render_device(full, out.data_ptr(), stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        stress = {"workload": "4000 displaced icospheres (20.48M triangles) in one homogeneous "
+                              "medium, 3840x2160, 256 spp, depth 16, reference builder",
+                  "ms": ms, "value": 3840 * 2160 * 256 / ms / 1e3, "unit": METRIC,
+                  "scene_create_s": build_s, "bvh_build_ms": 1e3 * big.build_seconds()}
+        big.close()
 
     peak, peak_kind = measured_peak()
     algorithmic = (BYTES_PER_BOUNDS_TEST * counted.bounds_tests +
@@ -553,7 +582,8 @@ def run_ours(args):
                                      "ms_per_step": 1e3 * plain_seconds,
                                      "engine": "mr_render_device, one job per call"},
                        "batched_vs_plain": value / plain_value,
-                       "serving": serving, "large_frame": large_frame},
+                       "serving": serving, "serving_sustainable": sustainable,
+                       "large_frame": large_frame, "stress": stress},
             "roofline": {"bound": "hbm", "kernel": "trace_kernel (nearest-hit + shadow "
                                                    "traversal), plain leg of the same jobs",
                          "achieved": achieved, "peak": peak, "peak_source": peak_kind,
