@@ -846,28 +846,43 @@ std::vector<std::shared_ptr<Workspace>> pool;
 
 }  // namespace
 
+// Workspaces are pooled per process: a request takes the smallest pooled workspace of its device
+// that is large enough in every dimension, and requests are rounded up (powers of two, bounces to
+// a multiple of 16) so that one workspace serves many job shapes. When more than four are pooled
+// the smallest goes: large ones serve every smaller request, so a stream of uneven jobs settles
+// on reuse instead of reallocating (a device-wide synchronising cudaFree each time).
 std::shared_ptr<Workspace> acquire_workspace(size_t capacity, uint32_t max_bounces, size_t pixels) {
     int device = 0;
     MR_CUDA(cudaGetDevice(&device));
+    const auto round_up = [](size_t v, size_t floor) {
+        size_t r = floor;
+        while (r < v) {
+            r <<= 1;
+        }
+        return r;
+    };
+    capacity    = round_up(capacity, size_t(1) << 16);
+    pixels      = pixels ? round_up(pixels, size_t(1) << 16) : 0;
+    max_bounces = (max_bounces + 15u) & ~15u;
     {
         std::lock_guard<std::mutex> lock(pool_mutex);
+        long best = -1;
         for (size_t i = 0; i < pool.size(); ++i) {
-            auto& w = pool[i];
-            int   d = -1;
-            cudaPointerAttributes attr{};
-            if (cudaPointerGetAttributes(&attr, w->memory) == cudaSuccess) {
-                d = attr.device;
-            }
-            if (d == device && w->capacity >= capacity && w->max_bounces >= max_bounces &&
-                w->pixels >= pixels) {
-                auto out = w;
-                pool.erase(pool.begin() + static_cast<long>(i));
-                return out;
+            const auto& w = pool[i];
+            if (w->device == device && w->capacity >= capacity && w->max_bounces >= max_bounces &&
+                w->pixels >= pixels && (best < 0 || w->bytes < pool[best]->bytes)) {
+                best = static_cast<long>(i);
             }
         }
+        if (best >= 0) {
+            auto out = pool[best];
+            pool.erase(pool.begin() + best);
+            return out;
+        }
     }
-    cudaGetLastError();
-    return allocate_workspace(capacity, max_bounces, pixels);
+    auto ws    = allocate_workspace(capacity, max_bounces, pixels);
+    ws->device = device;
+    return ws;
 }
 
 void release_workspace(std::shared_ptr<Workspace> ws) {
@@ -877,7 +892,10 @@ void release_workspace(std::shared_ptr<Workspace> ws) {
     std::lock_guard<std::mutex> lock(pool_mutex);
     pool.push_back(std::move(ws));
     if (pool.size() > 4) {
-        pool.erase(pool.begin());
+        auto smallest = std::min_element(pool.begin(), pool.end(), [](const auto& a, const auto& b) {
+            return a->bytes < b->bytes;
+        });
+        pool.erase(smallest);
     }
 }
 

@@ -115,6 +115,7 @@ struct Workspace {
     Queues    queues{};
     float4*   accumulator  = nullptr;  // Kahan sum per pixel (sum, compensation) of a frame
     size_t    pixels       = 0;
+    int       device       = 0;
     ~Workspace();
 };
 
