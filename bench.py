@@ -469,6 +469,25 @@ def run_ours(args):
     lib.mr_set_kernel_timing(0)
     plain_value = samples / plain_seconds / 1e6
 
+    # The smaller half of the mix (by samples), batched and plain: the jobs batching is for.
+    order = sorted(range(len(jobs)), key=lambda k: jobs[k].render.width * jobs[k].render.height *
+                   jobs[k].render.samples_per_pixel)
+    small = [jobs[k] for k in order[: len(jobs) // 2]]
+    small_samples = sum(j.render.width * j.render.height * j.render.samples_per_pixel for j in small)
+    _, _, info = api.render_batch(small, tuned, copy_images=False)
+    small_batched = info["device_seconds"]
+    e0.record(stream)
+    for j in small:
+        api.PathTracer(j.scene, j.integrator).render_device(j.render, image.data_ptr(),
+                                                            stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    small_plain = e0.elapsed_time(e1) / 1e3
+    small_jobs = {"jobs": len(small), "samples": small_samples,
+                  "batched": small_samples / small_batched / 1e6,
+                  "plain": small_samples / small_plain / 1e6,
+                  "batched_vs_plain": small_plain / small_batched, "unit": METRIC}
+
     # The single 1M-triangle frame (plain path), after one warm-up frame.
     large = api.Scene(sc.large_scene().snapshot())
     frame_render = api.RenderSettings(1920, 1080, 64, 1 + rank)
@@ -582,6 +601,7 @@ def run_ours(args):
                                      "ms_per_step": 1e3 * plain_seconds,
                                      "engine": "mr_render_device, one job per call"},
                        "batched_vs_plain": value / plain_value,
+                       "small_jobs": small_jobs,
                        "serving": serving, "serving_sustainable": sustainable,
                        "large_frame": large_frame, "stress": stress},
             "roofline": {"bound": "hbm", "kernel": "trace_kernel (nearest-hit + shadow "
