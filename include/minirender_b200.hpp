@@ -7,6 +7,7 @@
 // A status from the library is rethrown as the exception the reference would throw
 // (std::invalid_argument, std::out_of_range, std::overflow_error, std::logic_error,
 // std::length_error, std::runtime_error). Images are row-major linear RGB floats, origin top-left.
+// render_batch and RenderServer (many renders at once) have no reference counterpart.
 #pragma once
 
 #include <chrono>
@@ -101,11 +102,116 @@ class PathTracer {
                              radiance.data(), statistics));
         return radiance;
     }
+    // Rows [row_begin, row_end) of render(): bit for bit the full image's rows (row bands of
+    // one frame rendered by several ranks).
+    Image render_rows(const mr_render_settings& settings, uint64_t row_begin, uint64_t row_end,
+                      mr_path_statistics* statistics = nullptr) const {
+        Image image{static_cast<std::size_t>(settings.width),
+                    static_cast<std::size_t>(row_end > row_begin ? row_end - row_begin : 0), {}};
+        image.rgb.resize(3 * image.width * image.height);
+        check(mr_render_rows(scene_->get(), &settings_, &settings, row_begin, row_end,
+                             image.rgb.empty() ? nullptr : image.rgb.data(), statistics));
+        return image;
+    }
     const Scene& scene() const noexcept { return *scene_; }
+    const mr_integrator_settings& settings() const noexcept { return settings_; }
 
   private:
     std::shared_ptr<const Scene> scene_;
     mr_integrator_settings       settings_;
+};
+
+// Many renders at once (mr_render_batch; no reference counterpart): each image is bitwise the
+// one PathTracer::render gives alone. Throws the first failing job's exception.
+struct BatchJob {
+    std::shared_ptr<const Scene> scene;
+    mr_render_settings           render;
+    mr_integrator_settings       integrator{MR_SAMPLING_MIS, 8, 1, 3};
+};
+
+inline std::vector<Image> render_batch(const std::vector<BatchJob>& jobs,
+                                       const mr_batch_settings* settings = nullptr,
+                                       mr_batch_statistics* statistics = nullptr) {
+    std::vector<Image>        images(jobs.size());
+    std::vector<mr_batch_job> records(jobs.size());
+    for (std::size_t i = 0; i < jobs.size(); ++i) {
+        if (!jobs[i].scene) {
+            throw std::invalid_argument("Batch job requires a scene");
+        }
+        images[i].width  = static_cast<std::size_t>(jobs[i].render.width);
+        images[i].height = static_cast<std::size_t>(jobs[i].render.height);
+        images[i].rgb.resize(3 * images[i].width * images[i].height);
+        records[i] = {jobs[i].scene->get(), jobs[i].integrator, jobs[i].render, images[i].rgb.data(), MR_OK};
+    }
+    mr_batch_settings defaults{0, 0, 0, 0, 1, 0};
+    check(mr_render_batch(records.data(), records.size(), settings ? settings : &defaults, statistics));
+    return images;
+}
+
+// Request loop over the GPU (mr_server_*; no reference counterpart): jobs are admitted by HBM
+// budget, rendered together, and paused, resumed or cancelled per job. The scenes of submitted
+// jobs are kept alive here until the server is destroyed.
+class RenderServer {
+  public:
+    explicit RenderServer(const mr_server_settings* settings = nullptr) {
+        mr_server_settings defaults{};
+        defaults.batch.use_graphs = 1;
+        mr_server* s = nullptr;
+        check(mr_server_create(settings ? settings : &defaults, &s));
+        handle_.reset(s);
+    }
+    uint64_t submit(std::shared_ptr<const Scene> scene, const mr_render_settings& render,
+                    const mr_integrator_settings& integrator = {MR_SAMPLING_MIS, 8, 1, 3}) {
+        if (!scene) {
+            throw std::invalid_argument("Render job requires a scene");
+        }
+        uint64_t job = 0;
+        check(mr_server_submit(handle_.get(), scene->get(), &render, &integrator, &job));
+        sizes_.emplace_back(job, std::make_pair(render.width, render.height));
+        scenes_.push_back(std::move(scene));
+        return job;
+    }
+    bool pause(uint64_t job) {
+        int accepted = 0;
+        check(mr_server_pause(handle_.get(), job, &accepted));
+        return accepted != 0;
+    }
+    bool resume(uint64_t job) {
+        int accepted = 0;
+        check(mr_server_resume(handle_.get(), job, &accepted));
+        return accepted != 0;
+    }
+    void cancel(uint64_t job) { check(mr_server_cancel(handle_.get(), job)); }
+    bool wait_for(uint64_t job, std::chrono::milliseconds timeout) {
+        int done = 0;
+        check(mr_server_wait(handle_.get(), job, static_cast<uint32_t>(timeout.count()), &done));
+        return done != 0;
+    }
+    mr_job_info info(uint64_t job) {
+        mr_job_info i{};
+        check(mr_server_job_info(handle_.get(), job, &i));
+        return i;
+    }
+    Image result(uint64_t job) {
+        for (const auto& [id, size] : sizes_) {
+            if (id == job) {
+                Image image{static_cast<std::size_t>(size.first), static_cast<std::size_t>(size.second), {}};
+                image.rgb.resize(3 * image.width * image.height);
+                check(mr_server_result(handle_.get(), job, image.rgb.data(), image.rgb.size()));
+                return image;
+            }
+        }
+        throw std::out_of_range("Unknown job");
+    }
+    void release(uint64_t job) { check(mr_server_release(handle_.get(), job)); }
+
+  private:
+    struct Deleter {
+        void operator()(mr_server* s) const noexcept { mr_server_destroy(s); }
+    };
+    std::unique_ptr<mr_server, Deleter>                             handle_;
+    std::vector<std::pair<uint64_t, std::pair<uint64_t, uint64_t>>> sizes_;
+    std::vector<std::shared_ptr<const Scene>>                       scenes_;
 };
 
 class RenderSession {

@@ -14,6 +14,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 PROGRAM = r"""
 #include "minirender_b200.hpp"
+#include <algorithm>
 #include <cstdio>
 #include <stdexcept>
 
@@ -35,7 +36,18 @@ int main() {
         minirender_b200::PathTracer tracer(scene);
         auto image = tracer.render({8, 8, 4, 1});
         std::printf("rendered %zu x %zu mean %f\n", image.width, image.height, image.rgb[0]);
-        return 0;
+        auto band = tracer.render_rows({8, 8, 4, 1}, 2, 5);
+        auto batch = minirender_b200::render_batch({{scene, {8, 8, 4, 1}}, {scene, {5, 3, 2, 9}}});
+        minirender_b200::RenderServer server;
+        const uint64_t job = server.submit(scene, {8, 8, 4, 1});
+        if (!server.wait_for(job, std::chrono::milliseconds(60000))) return 4;
+        auto served = server.result(job);
+        server.release(job);
+        const bool same = band.rgb.size() == 3 * 8 * 3 &&
+                          std::equal(band.rgb.begin(), band.rgb.end(), image.rgb.begin() + 3 * 8 * 2) &&
+                          batch[0].rgb == image.rgb && served.rgb == image.rgb;
+        std::printf("batch and served images %s\n", same ? "match" : "differ");
+        return same ? 0 : 5;
     } catch (const std::runtime_error& e) {
         std::printf("runtime_error: %s\n", e.what());
         return 3;
@@ -60,6 +72,6 @@ def test_cpp_adapter_compiles_links_and_reports_errors():
         result = subprocess.run([exe], capture_output=True, text=True, timeout=120)
         if os.path.exists("/dev/nvidia0"):
             assert result.returncode == 0, result.stdout + result.stderr
-            assert "rendered 8 x 8" in result.stdout
+            assert "rendered 8 x 8" in result.stdout and "match" in result.stdout
         else:
             assert result.returncode == 3 and "CUDA" in result.stdout, result.stdout
