@@ -474,6 +474,7 @@ def run_ours(args):
                    jobs[k].render.samples_per_pixel)
     small = [jobs[k] for k in order[: len(jobs) // 2]]
     small_samples = sum(j.render.width * j.render.height * j.render.samples_per_pixel for j in small)
+    api.render_batch(small, tuned, copy_images=False)  # warm-up
     _, _, info = api.render_batch(small, tuned, copy_images=False)
     small_batched = info["device_seconds"]
     e0.record(stream)

@@ -69,6 +69,8 @@ struct Job {
     uint32_t           state = MR_JOB_QUEUED;
     bool               paused = false;
     bool               finishing = false;  // last wave retired, image being copied out
+    bool               released  = false;  // forgotten by the caller; erased once no wave holds it
+    uint32_t           inflight  = 0;      // enqueued waves carrying a piece of this job
     Cursor             issued, done;
     uint64_t           issued_samples = 0, done_samples = 0;
     int                slot = -1;
@@ -430,13 +432,20 @@ class Server {
         return samples;
     }
 
+    // A released job disappears from queries at once; its record is erased when no enqueued
+    // wave refers to it any more (a cancelled or failed job can still have waves in flight).
     void release(uint64_t id) {
         std::lock_guard<std::mutex> lock(mutex_);
         Job& j = find(id);
         if (!terminal(j.state)) {
             fail(MR_LOGIC_ERROR, "The job is still active");
         }
-        jobs_.erase(id);
+        j.released = true;
+        active_.erase(std::remove(active_.begin(), active_.end(), &j), active_.end());
+        queued_.erase(std::remove(queued_.begin(), queued_.end(), &j), queued_.end());
+        if (j.inflight == 0) {
+            jobs_.erase(id);
+        }
     }
 
     mr_server_statistics statistics() {
@@ -492,7 +501,7 @@ class Server {
 
     Job& find(uint64_t id) {
         auto it = jobs_.find(id);
-        if (it == jobs_.end()) {
+        if (it == jobs_.end() || it->second->released) {
             fail(MR_OUT_OF_RANGE, "Unknown job");
         }
         return *it->second;
@@ -691,6 +700,7 @@ class Server {
             j->issued = after;
             j->issued_samples += paths;
             rec.pieces.push_back({j, after, paths, after.sample >= j->spp});
+            ++j->inflight;
         }
         if (rec.pieces.empty()) {
             return false;
@@ -750,6 +760,10 @@ class Server {
         for (const Piece& piece : rec.pieces) {
             Job& j = *piece.job;
             stats_.samples += piece.paths;
+            if (--j.inflight == 0 && j.released) {
+                jobs_.erase(j.id);
+                continue;
+            }
             if (terminal(j.state)) {
                 continue;
             }
@@ -807,6 +821,13 @@ class Server {
                 for (auto& [id, job] : jobs_) {
                     if (!terminal(job->state) && !job->finishing) {
                         fail_locked(*job, e.status, e.what());
+                    }
+                }
+                for (WaveRecord& rec : inflight_) {
+                    for (const Piece& piece : rec.pieces) {
+                        if (--piece.job->inflight == 0 && piece.job->released) {
+                            jobs_.erase(piece.job->id);
+                        }
                     }
                 }
                 inflight_.clear();
@@ -918,7 +939,72 @@ const Scene* scene_ptr(const mr_scene* s) {
     return s->impl.get();
 }
 
-// Renders a job list through a private server; fills per-job statuses.
+// One server per device is kept between batch calls, so repeated calls with the same wave shape
+// reuse its lanes' path state and captured graphs instead of rebuilding them. A call takes it
+// only when no other call holds it (a concurrent call gets a private server) and a call with a
+// different shape replaces it. The cache lives until the process exits.
+struct CachedServer {
+    int                     device = -1;
+    mr_batch_settings       key{};
+    std::unique_ptr<Server> server;
+    bool                    busy = false;
+};
+
+std::mutex&                 server_cache_mutex() {
+    static std::mutex* m = new std::mutex;
+    return *m;
+}
+std::vector<CachedServer>&  server_cache() {
+    static auto* cache = new std::vector<CachedServer>;  // never destroyed: see above
+    return *cache;
+}
+
+bool same_shape(const mr_batch_settings& a, const mr_batch_settings& b) {
+    return a.wave_paths == b.wave_paths && a.trace_blocks_per_sm == b.trace_blocks_per_sm &&
+           a.shade_blocks_per_sm == b.shade_blocks_per_sm && a.sort_threshold == b.sort_threshold &&
+           a.use_graphs == b.use_graphs && a.concurrent_waves == b.concurrent_waves;
+}
+
+// The cached server of the current device for `shape`, marked busy, or null when another call
+// holds it.
+Server* take_cached_server(const mr_server_settings& ss, size_t& slot) {
+    int device = 0;
+    MR_CUDA(cudaGetDevice(&device));
+    std::lock_guard<std::mutex> lock(server_cache_mutex());
+    auto& cache = server_cache();
+    for (size_t i = 0; i < cache.size(); ++i) {
+        CachedServer& c = cache[i];
+        if (c.device != device) {
+            continue;
+        }
+        if (c.busy) {
+            return nullptr;
+        }
+        if (!same_shape(c.key, ss.batch)) {
+            c.server.reset();
+            c.server = std::make_unique<Server>(ss);
+            c.key    = ss.batch;
+        }
+        c.busy = true;
+        slot   = i;
+        return c.server.get();
+    }
+    CachedServer c;
+    c.device = device;
+    c.key    = ss.batch;
+    c.server = std::make_unique<Server>(ss);
+    c.busy   = true;
+    cache.push_back(std::move(c));
+    slot = cache.size() - 1;
+    return cache.back().server.get();
+}
+
+void return_cached_server(size_t slot) {
+    std::lock_guard<std::mutex> lock(server_cache_mutex());
+    server_cache()[slot].busy = false;
+}
+
+// Renders a job list on the device's cached server (or a private one); fills per-job statuses.
 mr_status run_batch(mr_batch_job* jobs, size_t count, const mr_batch_settings* settings,
                     mr_batch_statistics* statistics, bool copy_images) {
     require(jobs != nullptr || count == 0, "Job list is null");
@@ -932,12 +1018,29 @@ mr_status run_batch(mr_batch_job* jobs, size_t count, const mr_batch_settings* s
     size_t free_bytes = 0, total_bytes = 0;
     MR_CUDA(cudaMemGetInfo(&free_bytes, &total_bytes));
     ss.hbm_budget_bytes = free_bytes / 10 * 8;
-    ss.max_jobs         = static_cast<uint32_t>(std::min<size_t>(std::max<size_t>(count, 1), 4096));
+    ss.max_jobs         = 4096;
     for (size_t i = 0; i < count; ++i) {
         jobs[i].status = MR_OK;
     }
-    const auto t0 = Clock::now();
-    Server     server(ss);
+    const auto              t0 = Clock::now();
+    size_t                  slot = 0;
+    std::unique_ptr<Server> private_server;
+    Server*                 cached = take_cached_server(ss, slot);
+    if (!cached) {
+        private_server = std::make_unique<Server>(ss);
+    }
+    struct Return {
+        Server* cached;
+        size_t  slot;
+        ~Return() {
+            if (cached) {
+                return_cached_server(slot);
+            }
+        }
+    } give_back{cached, slot};
+    Server& server = cached ? *cached : *private_server;
+    const mr_server_statistics stats_before = server.statistics();
+    const mr_path_statistics   paths_before = server.path_statistics();
     cudaEvent_t marks[2] = {nullptr, nullptr};
     MR_CUDA(cudaEventCreate(&marks[0]));
     MR_CUDA(cudaEventCreate(&marks[1]));
@@ -976,19 +1079,30 @@ mr_status run_batch(mr_batch_job* jobs, size_t count, const mr_batch_settings* s
                 set_last_error(info.error);
             }
         }
+        server.release(ids[i]);
     }
     if (statistics) {
         const mr_server_statistics s = server.statistics();
+        const mr_path_statistics   p = server.path_statistics();
         std::memset(statistics, 0, sizeof(*statistics));
-        statistics->waves           = s.waves;
-        statistics->segments        = s.segments;
-        statistics->samples         = s.samples;
-        statistics->kernel_launches = s.kernel_launches;
-        statistics->graph_launches  = s.graph_launches;
+        statistics->waves           = s.waves - stats_before.waves;
+        statistics->segments        = s.segments - stats_before.segments;
+        statistics->samples         = s.samples - stats_before.samples;
+        statistics->kernel_launches = s.kernel_launches - stats_before.kernel_launches;
+        statistics->graph_launches  = s.graph_launches - stats_before.graph_launches;
         statistics->seconds         = seconds;
-        statistics->busy_seconds    = s.busy_seconds;
+        statistics->busy_seconds    = s.busy_seconds - stats_before.busy_seconds;
         statistics->device_seconds  = device_ms * 1e-3;
-        statistics->paths           = server.path_statistics();
+        statistics->paths.paths                    = p.paths - paths_before.paths;
+        statistics->paths.shadow_rays              = p.shadow_rays - paths_before.shadow_rays;
+        statistics->paths.scattering_events        = p.scattering_events - paths_before.scattering_events;
+        statistics->paths.roulette_terminations    = p.roulette_terminations - paths_before.roulette_terminations;
+        statistics->paths.medium_scattering_events =
+            p.medium_scattering_events - paths_before.medium_scattering_events;
+        statistics->paths.geometry.bounds_tests =
+            p.geometry.bounds_tests - paths_before.geometry.bounds_tests;
+        statistics->paths.geometry.triangle_tests =
+            p.geometry.triangle_tests - paths_before.geometry.triangle_tests;
     }
     return first;
 }

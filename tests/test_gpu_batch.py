@@ -192,3 +192,30 @@ def test_row_bands_assemble_the_frame_bitwise(api, scenes):
     assert tracer.render_rows(render, 5, 5).shape == (0, 83, 3)
     with pytest.raises(api.MiniRenderError):
         tracer.render_rows(render, 10, 62)
+
+
+def test_repeated_batches_reuse_the_engine_and_report_per_call(api, scenes):
+    jobs = job_mix(api, scenes)
+    settings = api.BatchSettings(wave_paths=4096, concurrent_waves=2)
+    first, codes, a = api.render_batch(jobs, settings)
+    second, codes2, b = api.render_batch(jobs, settings)
+    assert codes == codes2 == [0] * len(jobs)
+    assert a["samples"] == b["samples"] and a["waves"] == b["waves"]  # per-call figures
+    assert a["paths"]["paths"] == b["paths"]["paths"]
+    for x, y in zip(first, second):
+        np.testing.assert_array_equal(x, y)
+
+
+def test_released_cancelled_job_is_forgotten_safely(api, scenes):
+    R = api.RenderSettings
+    with api.RenderServer(batch=api.BatchSettings(wave_paths=4096)) as server:
+        victim = server.submit(scenes[2], R(128, 128, 32, 8))
+        other = server.submit(scenes[1], R(64, 64, 8, 9))
+        time.sleep(0.01)
+        server.cancel(victim)
+        server.release(victim)  # waves carrying it may still be in flight
+        with pytest.raises(api.MiniRenderError):
+            server.info(victim)
+        assert server.wait(other, 60_000)
+        np.testing.assert_array_equal(server.result(other),
+                                      plain(api, api.BatchJob(scenes[1], R(64, 64, 8, 9))))
