@@ -1,0 +1,162 @@
+"""Scene JSON v1 and OBJ ingestion (src/assets/scene_io.cpp:45-160, src/assets/obj_loader.cpp):
+keys, defaults, id references, quad triangulation along the shorter diagonal, corner normals and
+the reference's rejections; generated scenes round-trip; the reference's own scene files load
+(when its tree is present) and the oracle renders one."""
+
+import json
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+from minirender_b200 import scene as sc
+from minirender_b200 import scene_io
+
+REFERENCE_SCENES = "/root/reference/scenes"
+
+
+def write(directory, name, text):
+    path = os.path.join(directory, name)
+    with open(path, "w") as f:
+        f.write(text)
+    return path
+
+
+def test_obj_corners_normals_and_triangulation():
+    with tempfile.TemporaryDirectory() as d:
+        path = write(d, "m.obj", "\n".join([
+            "# quad whose 0-2 diagonal is shorter, a quad whose 1-3 diagonal is, a triangle",
+            "v 0 0 0", "v 2 0 0", "v 2.5 1 0", "v 0.5 1 0",      # 0-2 longer than 1-3
+            "v 0 0 1", "v 1 0 1", "v 1 3 1", "v 0 1 1",          # 0-2 longer too; see below
+            "vn 0 0 2", "vt 0.25 0.5",
+            "o shape", "g group", "s 1", "usemtl anything",
+            "f 1 2 3 4",
+            "f 5/1 6/1 7/1 8/1",
+            "f -3//1 -2//1 -1//1",
+        ]))
+        mesh = scene_io.load_obj(path)
+    p = mesh.positions
+    assert p.shape == (8, 3) and mesh.triangle_count == 5
+    d02 = np.sum((p[2] - p[0]) ** 2); d13 = np.sum((p[3] - p[1]) ** 2)
+    expected = [[0, 1, 2], [0, 2, 3]] if d02 < d13 else [[0, 1, 3], [1, 2, 3]]
+    assert mesh.corner_positions[:2].tolist() == expected
+    d02 = np.sum((p[6] - p[4]) ** 2); d13 = np.sum((p[7] - p[5]) ** 2)
+    expected = [[4, 5, 6], [4, 6, 7]] if d02 < d13 else [[4, 5, 7], [5, 6, 7]]
+    assert mesh.corner_positions[2:4].tolist() == expected
+    assert mesh.corner_positions[4].tolist() == [5, 6, 7]  # relative indices
+    assert np.allclose(mesh.corner_normals[4], [0, 0, 1])  # vn normalised
+    assert np.allclose(mesh.corner_normals[0], [0, 0, 1])  # geometric normal without vn
+    assert np.allclose(mesh.corner_uvs[2], [[0.25, 0.5]] * 3)
+    assert np.allclose(mesh.corner_uvs[0], 0)
+
+
+@pytest.mark.parametrize("body,message", [
+    ("v 0 0 0\nv 1 0 0\nv 2 0 0\nf 1 2 3\n", "degenerate"),
+    ("v 0 0 0\nv 1 0 0\nv 0 1 0\nf 1 2 4\n", "vertex index"),
+    ("v 0 0 0\nv 1 0 0\nv 0 1 0\nvn 0 0 0\nf 1//1 2//1 3//1\n", "normal is zero"),
+])
+def test_obj_rejections(body, message):
+    with tempfile.TemporaryDirectory() as d:
+        with pytest.raises(ValueError, match=message):
+            scene_io.load_obj(write(d, "bad.obj", body))
+
+
+def minimal_scene(**overrides):
+    data = {
+        "version": 1,
+        "camera": {"position": [0, 1, 3], "target": [0, 1, 0], "up": [0, 1, 0],
+                   "vertical_fov": 40, "near": 0.05, "far": 50},
+        "environment": [0.1, 0.2, 0.3],
+        "materials": [{"id": "white", "kind": "diffuse", "base_color": [0.7, 0.7, 0.7]},
+                      {"id": "lamp", "kind": "diffuse", "base_color": [0, 0, 0],
+                       "emission": [5, 5, 5], "double_sided": False}],
+        "meshes": [{"id": "plane", "source": "plane.obj"}],
+        "objects": [{"id": "floor", "mesh": "plane", "material": "white",
+                     "transform": {"translation": [0, 0, 0], "rotation": [0, 0, 0],
+                                   "scale": [1, 1, 1]}},
+                    {"id": "light", "mesh": "plane", "material": "lamp", "visible": True,
+                     "transform": {"translation": [0, 2, 0], "rotation": [180, 0, 0],
+                                   "scale": [0.2, 1, 0.2]}}],
+        "directional_lights": [{"id": "sun", "direction": [0, -1, 0], "color": [1, 1, 1],
+                                "intensity": 2}],
+    }
+    data.update(overrides)
+    return data
+
+
+PLANE = "v -1 0 -1\nv -1 0 1\nv 1 0 1\nv 1 0 -1\nf 1 2 3 4\n"
+
+
+def test_scene_keys_defaults_and_references():
+    with tempfile.TemporaryDirectory() as d:
+        write(d, "plane.obj", PLANE)
+        data = minimal_scene(media=[{"id": "fog", "minimum": [-1, 0, -1], "maximum": [1, 2, 1],
+                                     "absorption": [0.1, 0.2, 0.3], "scattering": [0.4, 0.4, 0.4],
+                                     "anisotropy": 0.25}])
+        doc = scene_io.load_scene(write(d, "s.json", json.dumps(data)))
+    assert doc.camera.aperture_radius == 0.0 and doc.camera.focus_distance == 4.0
+    assert doc.materials[0].roughness == pytest.approx(0.35) and doc.materials[0].ior == 1.5
+    assert doc.materials[0].double_sided and not doc.materials[1].double_sided
+    assert doc.materials[0].emission == (0.0, 0.0, 0.0)
+    assert [o.mesh for o in doc.objects] == [0, 0] and [o.material for o in doc.objects] == [0, 1]
+    assert doc.media[0].enabled and doc.media[0].anisotropy == 0.25
+    assert doc.directional_lights[0].intensity == 2.0
+    assert doc.snapshot().triangle_count == 4
+
+
+@pytest.mark.parametrize("change,message", [
+    ({"version": 2}, "version"),
+    ({"objects": [{"id": "x", "mesh": "nope", "material": "white",
+                   "transform": {"translation": [0, 0, 0], "rotation": [0, 0, 0],
+                                 "scale": [1, 1, 1]}}]}, "missing mesh"),
+    ({"materials": [{"id": "white", "kind": "plastic", "base_color": [1, 1, 1]}]}, "kind"),
+    ({"materials": [{"id": "white", "kind": "diffuse", "base_color": [1, 1, 1],
+                     "base_color_texture": "wood"}]}, "textures"),
+    ({"environment_map": {"texture": "sky"}}, "Environment maps"),
+    ({"camera": {"position": [0, 1, 3]}}, "missing key"),
+])
+def test_scene_rejections(change, message):
+    with tempfile.TemporaryDirectory() as d:
+        write(d, "plane.obj", PLANE)
+        with pytest.raises(ValueError, match=message):
+            scene_io.load_scene(write(d, "s.json", json.dumps(minimal_scene(**change))))
+
+
+def test_generated_scene_round_trips(oracle):
+    doc = sc.cornell_box()
+    doc.media = [sc.MediumRegion((-0.5, 0, -0.5), (0.5, 1, 0.5), (0.1, 0.1, 0.1), (0.3, 0.3, 0.3), 0.2)]
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "cornell.json")
+        scene_io.save_scene(doc, path)
+        back = scene_io.load_scene(path)
+    a, b = doc.snapshot(), back.snapshot()
+    assert np.array_equal(a.world_triangles(), b.world_triangles())
+    from minirender_b200 import _abi
+    render = _abi.RenderSettings(12, 9, 2, 4)
+    settings = oracle.integrator("mis", 4, True, 3)
+    ia, _ = oracle.OracleScene(a, settings).render(render, threads=2)
+    ib, _ = oracle.OracleScene(b, settings).render(render, threads=2)
+    assert np.array_equal(ia, ib)
+
+
+@pytest.mark.skipif(not os.path.isdir(REFERENCE_SCENES), reason="reference scenes not present")
+def test_reference_scene_files_load(oracle):
+    loaded = 0
+    for name in sorted(os.listdir(REFERENCE_SCENES)):
+        if not name.endswith(".json") or name == "resource_catalog.json":
+            continue
+        path = os.path.join(REFERENCE_SCENES, name)
+        try:
+            doc = scene_io.load_scene(path)
+        except ValueError as e:
+            assert "textures" in str(e) or "Environment maps" in str(e), (name, e)
+            continue
+        assert doc.snapshot().triangle_count > 0
+        loaded += 1
+    assert loaded >= 15
+    from minirender_b200 import _abi
+    doc = scene_io.load_scene(os.path.join(REFERENCE_SCENES, "cornell-box.json"))
+    image, stats = oracle.OracleScene(doc.snapshot(), oracle.integrator("mis", 4, True, 3)).render(
+        _abi.RenderSettings(16, 12, 2, 1), threads=2)
+    assert np.isfinite(image).all() and image.mean() > 0 and stats["paths"] == 16 * 12 * 2
