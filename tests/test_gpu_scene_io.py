@@ -31,3 +31,29 @@ def test_loaded_scene_renders_like_the_oracle(oracle):
     ok = np.all(np.abs(gpu - cpu) <= 2e-3 * np.maximum(cpu, 0.05 * scale), axis=2)
     assert ok.mean() >= 0.99, ok.mean()
     assert gpu.mean() == pytest.approx(cpu.mean(), rel=5e-3)
+
+
+def test_render_command_writes_the_session_image(tmp_path):
+    import subprocess
+    import sys
+    from minirender_b200 import api, image_io
+    from tests.test_image_io import read_exr, read_png
+    doc = sc.cornell_box()
+    scene_path = tmp_path / "cornell.json"
+    scene_io.save_scene(doc, str(scene_path))
+    out = tmp_path / "renders" / "cornell.png"
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    result = subprocess.run([sys.executable, "-m", "minirender_b200.render_cli", "--render",
+                             str(scene_path), str(out), "--width", "32", "--height", "24",
+                             "--spp", "4", "--seed", "3", "--depth", "6", "--exposure", "0.5"],
+                            capture_output=True, text=True, cwd=root, timeout=300)
+    assert result.returncode == 0, result.stderr
+    assert "EXR and PNG saved." in result.stdout and "paths: 3072" in result.stdout
+    exr, _ = read_exr(str(tmp_path / "renders" / "cornell.exr"))
+    png = read_png(str(tmp_path / "renders" / "cornell.png"))
+    expected, _ = api.PathTracer(scene_io.load_scene(str(scene_path)).snapshot(),
+                                 api.IntegratorSettings("mis", 6, True, 3)).render(
+        api.RenderSettings(32, 24, 4, 3))
+    assert np.array_equal(exr, expected)
+    display = api.display_image(expected, 0.5)
+    assert np.array_equal(png, image_io.encode_unorm8(image_io.linear_to_srgb(display)))
