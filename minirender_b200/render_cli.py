@@ -6,7 +6,8 @@ is dropped), options ``--width --height --spp --depth --mode mis|bsdf|light --se
 --no-rr --rr-depth --threads --tile --batch``; the render runs as a RenderSession with progress
 lines on stderr, then ``prefix.exr`` (linear) and ``prefix.png`` (display_image with the exposure,
 sRGB) are written and the statistics printed. ``--integrator sppm`` and its options are rejected:
-SPPM is not part of this path tracer.
+SPPM is not part of this path tracer. ``--trace-normals scene.json out.png`` is the geometry
+diagnostic of src/app/cli.cpp:60-97.
 """
 
 from __future__ import annotations
@@ -118,11 +119,82 @@ def run(argv: list[str]) -> int:
     return 0
 
 
+def trace_normals(scene_path: str, output: str) -> int:
+    """The --trace-normals geometry diagnostic (src/app/cli.cpp:60-97): one primary ray through
+    each pixel centre of a 256x256 image (pinhole, aspect 1, clip interval near/cos..far/cos),
+    the world-space shading normal of the nearest hit mapped to n * 0.5 + 0.5 (black on a miss),
+    written as PNG, with the BVH statistics, build and trace times and the query counters."""
+    import numpy as np
+    doc = load_scene(scene_path)
+    snap = doc.snapshot()
+    start = time.perf_counter()
+    scene = api.Scene(snap)
+    built = time.perf_counter()
+    size = 256
+    c = doc.camera
+    f32 = np.float32
+    position = np.asarray(c.position, f32)
+    forward = np.asarray(c.target, f32) - position
+    forward = (forward / np.linalg.norm(forward)).astype(f32)
+    right = np.cross(forward, np.asarray(c.up, f32))
+    right = (right / np.linalg.norm(right)).astype(f32)
+    up = np.cross(right, forward).astype(f32)
+    half = f32(np.tan(np.radians(c.vertical_fov_degrees) * 0.5))
+    centres = (np.arange(size, dtype=f32) + f32(0.5)) / f32(size)
+    v, u = np.meshgrid(centres, centres, indexing="ij")
+    d = (forward + ((f32(2) * u - f32(1)) * half)[..., None] * right +
+         ((f32(1) - f32(2) * v) * half)[..., None] * up).reshape(-1, 3)
+    d = (d / np.linalg.norm(d, axis=1, keepdims=True)).astype(f32)
+    cosine = d @ forward
+    hits, counters = scene.intersect(np.broadcast_to(position, d.shape), d,
+                                     c.near_plane / cosine, c.far_plane / cosine)
+    # SceneBvh::surface_hit's shading normal (src/render/bvh.cpp:412-440): barycentric sum of
+    # the unit world corner normals, oriented to the geometric normal's side.
+    visible = [o for o in doc.objects if o.visible]
+    image = np.zeros((size * size, 3), f32)
+    world = snap.world_triangles().astype(np.float64)
+    hit = np.nonzero(hits["primitive"] != 0xFFFFFFFF)[0]
+    for i in hit:
+        obj = visible[int(hits["instance"][i])]
+        mesh = doc.meshes[obj.mesh]
+        n_to_w = obj.transform.normal_matrix().astype(np.float64).T  # column-major storage
+        corners = mesh.corner_normals[int(hits["triangle"][i])].astype(np.float64)
+        tri = world[int(hits["primitive"][i])]
+        geometric = np.cross(tri[1] - tri[0], tri[2] - tri[0])
+        geometric /= np.linalg.norm(geometric)
+        if np.linalg.det(obj.transform.matrix()[:3, :3].astype(np.float64)) < 0:
+            geometric = -geometric
+        shading = np.zeros(3)
+        for k in range(3):
+            w = n_to_w @ corners[k]
+            shading += float(hits["barycentric"][i][k]) * w / np.linalg.norm(w)
+        if shading @ shading < 1e-24:
+            shading = geometric
+        else:
+            shading /= np.linalg.norm(shading)
+            if shading @ geometric < 0:
+                shading = -shading
+        image[i] = shading * 0.5 + 0.5
+    finished = time.perf_counter()
+    write_png(output, image.reshape(size, size, 3))
+    stats = scene.statistics()
+    print(f"geometry diagnostic: world-space shading normals\ntriangles: {stats['triangles']}\n"
+          f"nodes: {stats['nodes']}\nleaves: {stats['leaves']}\n"
+          f"maximum depth: {stats['maximum_depth']}\nbuild ms: {1e3 * (built - start):.3f}\n"
+          f"trace ms: {1e3 * (finished - built):.3f}\n"
+          f"bounds tests: {counters['bounds_tests']}\ntriangle tests: {counters['triangle_tests']}")
+    return 0
+
+
 def main() -> int:
     args = sys.argv[1:]
-    if args and args[0] == "--render":
-        args = args[1:]
     try:
+        if args and args[0] == "--trace-normals":
+            if len(args) != 3:
+                raise ValueError("Usage: --trace-normals scene.json output.png")
+            return trace_normals(args[1], args[2])
+        if args and args[0] == "--render":
+            args = args[1:]
         return run(args)
     except (ValueError, RuntimeError, api.MiniRenderError) as error:
         print(f"error: {error}", file=sys.stderr)

@@ -57,3 +57,27 @@ def test_render_command_writes_the_session_image(tmp_path):
     assert np.array_equal(exr, expected)
     display = api.display_image(expected, 0.5)
     assert np.array_equal(png, image_io.encode_unorm8(image_io.linear_to_srgb(display)))
+
+
+def test_trace_normals_diagnostic(tmp_path):
+    import subprocess
+    import sys
+    from tests.test_image_io import read_png
+    scene_path = tmp_path / "cornell.json"
+    scene_io.save_scene(sc.cornell_box(), str(scene_path))
+    out = tmp_path / "normals.png"
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    result = subprocess.run([sys.executable, "-m", "minirender_b200.render_cli", "--trace-normals",
+                             str(scene_path), str(out)], capture_output=True, text=True, cwd=root,
+                            timeout=300)
+    assert result.returncode == 0, result.stderr
+    assert "triangles: 36" in result.stdout and "bounds tests:" in result.stdout
+    image = read_png(str(out))
+    assert image.shape == (256, 256, 3)
+    # The centre of the image looks at the back wall or a box: a hit with a unit normal.
+    from minirender_b200 import image_io
+    centre = image[128, 128].astype(int)
+    assert centre.sum() > 0
+    # The floor near the bottom centre faces +y: normal (0, 1, 0) -> (0.5, 1, 0.5).
+    expected = image_io.encode_unorm8(image_io.linear_to_srgb(np.array([0.5, 1.0, 0.5], np.float32)))
+    assert np.abs(image[250, 128].astype(int) - expected.astype(int)).max() <= 1
