@@ -98,7 +98,7 @@ def trace_sample(k):
     image = torch.empty(job["width"] * job["height"] * 3, dtype=torch.float32, device="cuda")
     lib = _abi.load_library()
     assert lib.mr_set_kernel_timing(1) == 0
-    tracer.render_device(render, image.data_ptr())
+    stats = tracer.render_device(render, image.data_ptr(), statistics=True)
     torch.cuda.synchronize()
     launches, seconds, all_launches = C.c_uint64(), C.c_double(), C.c_uint64()
     counted = _abi.TraceStatistics()
@@ -106,7 +106,10 @@ def trace_sample(k):
     lib.mr_set_kernel_timing(0)
     algorithmic = (BYTES_PER_BOUNDS_TEST * counted.bounds_tests +
                    BYTES_PER_TRIANGLE_TEST * counted.triangle_tests)
+    # Rays traced: camera rays, one extension ray per continued scattering event, shadow rays.
+    rays = stats["paths"] + stats["scattering_events"] + stats["shadow_rays"]
     print(json.dumps({"job": k, **job, "trace_launches": launches.value,
+                      "rays": rays, "rays_per_second": rays / seconds.value,
                       "bounds_tests": counted.bounds_tests,
                       "triangle_tests": counted.triangle_tests,
                       "algorithmic_bytes": algorithmic, "trace_seconds": seconds.value,
