@@ -106,8 +106,10 @@ def trace_sample(k):
     lib.mr_set_kernel_timing(0)
     algorithmic = (BYTES_PER_BOUNDS_TEST * counted.bounds_tests +
                    BYTES_PER_TRIANGLE_TEST * counted.triangle_tests)
-    # Rays traced: camera rays, one extension ray per continued scattering event, shadow rays.
-    rays = stats["paths"] + stats["scattering_events"] + stats["shadow_rays"]
+    # Rays traced: camera rays, an extension ray per scattering event that survived roulette,
+    # shadow rays.
+    rays = (stats["paths"] + stats["scattering_events"] - stats["roulette_terminations"] +
+            stats["shadow_rays"])
     print(json.dumps({"job": k, **job, "trace_launches": launches.value,
                       "rays": rays, "rays_per_second": rays / seconds.value,
                       "bounds_tests": counted.bounds_tests,
