@@ -1,0 +1,25 @@
+"""bench.py's reference arm (the CPU oracle on the host cores) prints one JSON line with the
+contract's keys; run on a small budget here."""
+
+import json
+import os
+import subprocess
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_reference_arm_prints_the_contract_line():
+    env = dict(os.environ, BENCH_REFERENCE_SECONDS="2")
+    result = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--steps", "1",
+                             "--warmup", "1", "--jobs", "8"], cwd=ROOT, env=env,
+                            capture_output=True, text=True, timeout=600)
+    assert result.returncode == 0, result.stderr
+    line = json.loads(result.stdout.strip().splitlines()[-1])
+    for key in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step",
+                "higher_is_better", "scaling", "vs_baseline", "dtype", "data", "config"):
+        assert key in line, key
+    assert line["impl"] == "reference" and line["value"] > 0
+    assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] >= 1
+    assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["value"] == line["value"]
+    assert "workload" in line["config"]
