@@ -477,3 +477,21 @@ def test_gpu_builder_sah_within_two_percent(api, oracle, name):
     b, _ = imported.intersect(origins, d, 0, np.inf)
     assert np.array_equal(a["primitive"], b["primitive"])
     assert np.array_equal(a["distance"], b["distance"])
+
+
+@pytest.mark.parametrize("mode,rr", [("bsdf", True), ("light", True), ("mis", False),
+                                     ("light", False)])
+@pytest.mark.parametrize("name", ["cornell", "room"])
+def test_image_matches_oracle_for_every_sampling_mode(api, oracle, name, mode, rr):
+    doc = sc.cornell_box() if name == "cornell" else sc.job_scene(6_000, 31)
+    settings = api.IntegratorSettings(mode, 6, rr, 2)
+    g, o, snap = gpu_and_oracle(api, oracle, doc, settings=oracle.integrator(mode, 6, rr, 2))
+    render = api.RenderSettings(64, 48, 6, 11)
+    gpu, gstats = api.PathTracer(g, settings).render(render)
+    cpu, cstats = o.render(render.c())
+    scale = max(cpu.mean(), 1e-6)
+    tol = 2e-3 * np.maximum(cpu, 0.05 * scale)
+    ok = np.all(np.abs(gpu - cpu) <= tol, axis=2)
+    assert ok.mean() >= 0.99, ok.mean()
+    assert gpu.mean() == pytest.approx(cpu.mean(), rel=5e-3)
+    assert gstats["shadow_rays"] == pytest.approx(cstats["shadow_rays"], rel=2e-3)
