@@ -74,10 +74,21 @@ __device__ __forceinline__ float slab_enter(const RayQuery& q, float4 xy, float 
     return enter <= leave ? enter : __int_as_float(0x7fffffff);
 }
 
-// Slab test of one child of a wide node (six scalar bounds); NaN when missed.
-__device__ __forceinline__ float slab_enter6(const RayQuery& q, float lx, float hx, float ly, float hy,
-                                             float lz, float hz, float tmin, float tmax) {
-    return slab_enter(q, make_float4(lx, hx, ly, hy), lz, hz, tmin, tmax);
+// Slab test of one child of a wide node from its near and far planes per axis (already chosen by
+// the ray's direction signs): the entry distance, or +inf when missed. A hit's entry is at most
+// `tmax` (leave <= tmax), and +inf is also what an unbounded entry means, so interior traversal
+// treats +inf as "no child" without a second comparison against the interval.
+__device__ __forceinline__ float slab_near_far(const RayQuery& q, float nx, float fx, float ny, float fy,
+                                               float nz, float fz, float tmin, float tmax) {
+    const float tnx = (nx - q.o.x) * q.inv_lo[0];
+    const float tfx = (fx - q.o.x) * q.inv_hi[0];
+    const float tny = (ny - q.o.y) * q.inv_lo[1];
+    const float tfy = (fy - q.o.y) * q.inv_hi[1];
+    const float tnz = (nz - q.o.z) * q.inv_lo[2];
+    const float tfz = (fz - q.o.z) * q.inv_hi[2];
+    const float enter = fmaxf(fmaxf(tmin, tnx), fmaxf(tny, tnz));
+    const float leave = fminf(fminf(tmax, tfx), fminf(tfy, tfz));
+    return enter <= leave ? enter : __int_as_float(0x7f800000);
 }
 
 __device__ __forceinline__ void order2(float& ta, int& ra, float& tb, int& rb) {
@@ -191,6 +202,9 @@ __device__ __forceinline__ TraceResult trace(const DeviceScene& s, const RayQuer
     bool     held   = false;   // a postponed leaf in `leaf`
     uint32_t visits = 0;
     const float inf = __int_as_float(0x7f800000);
+    // Node rows 0..5 are lo.x, hi.x, lo.y, hi.y, lo.z, hi.z of the four children: the near plane
+    // of an axis is its hi row when the direction is negative there.
+    const int near_x = q.neg[0] ? 1 : 0, near_y = q.neg[1] ? 3 : 2, near_z = q.neg[2] ? 5 : 4;
     // Next stacked subtree that can still contain a nearer hit, or none.
     const auto pop = [&]() {
         while (sp > 0) {
@@ -217,19 +231,15 @@ __device__ __forceinline__ TraceResult trace(const DeviceScene& s, const RayQuer
                 return result;
             }
             const float4* n   = s.nodes + 8 * static_cast<size_t>(node);
-            const float4  lox = __ldg(n + 0), hix = __ldg(n + 1);
-            const float4  loy = __ldg(n + 2), hiy = __ldg(n + 3);
-            const float4  loz = __ldg(n + 4), hiz = __ldg(n + 5);
+            const float4  nx  = __ldg(n + near_x), fx = __ldg(n + (near_x ^ 1));
+            const float4  ny  = __ldg(n + near_y), fy = __ldg(n + (near_y ^ 1));
+            const float4  nz  = __ldg(n + near_z), fz = __ldg(n + (near_z ^ 1));
             const int4    ref = __ldg(reinterpret_cast<const int4*>(n + 6));
             counters.bounds += static_cast<uint32_t>(__ldg(reinterpret_cast<const int*>(n + 7)));
-            float t0 = slab_enter6(q, lox.x, hix.x, loy.x, hiy.x, loz.x, hiz.x, tmin, result.t);
-            float t1 = slab_enter6(q, lox.y, hix.y, loy.y, hiy.y, loz.y, hiz.y, tmin, result.t);
-            float t2 = slab_enter6(q, lox.z, hix.z, loy.z, hiy.z, loz.z, hiz.z, tmin, result.t);
-            float t3 = slab_enter6(q, lox.w, hix.w, loy.w, hiy.w, loz.w, hiz.w, tmin, result.t);
-            t0 = t0 <= result.t ? t0 : inf;
-            t1 = t1 <= result.t ? t1 : inf;
-            t2 = t2 <= result.t ? t2 : inf;
-            t3 = t3 <= result.t ? t3 : inf;
+            float t0 = slab_near_far(q, nx.x, fx.x, ny.x, fy.x, nz.x, fz.x, tmin, result.t);
+            float t1 = slab_near_far(q, nx.y, fx.y, ny.y, fy.y, nz.y, fz.y, tmin, result.t);
+            float t2 = slab_near_far(q, nx.z, fx.z, ny.z, fy.z, nz.z, fz.z, tmin, result.t);
+            float t3 = slab_near_far(q, nx.w, fx.w, ny.w, fy.w, nz.w, fz.w, tmin, result.t);
             int r0 = ref.x, r1 = ref.y, r2 = ref.z, r3 = ref.w;
             order2(t0, r0, t1, r1);
             order2(t2, r2, t3, r3);
