@@ -511,7 +511,7 @@ def run_ours(args):
     large.close()
 
     # End to end through the public API from pinned host memory.
-    e2e_value, h2d, d2h = None, 0, 0
+    e2e_value, h2d, d2h, e2e_phase = None, 0, 0, None
     if not args.no_e2e:
         h2d = sum(pin_snapshot(s) for s in snaps)
         d2h = sum(j.render.width * j.render.height * 3 * 4 for j in jobs)
@@ -519,19 +519,26 @@ def run_ours(args):
         from concurrent.futures import ThreadPoolExecutor
         builders = ThreadPoolExecutor(8)
 
+        phase = {"build": 0.0, "render": 0.0}
+
         def e2e_step():
             # Scenes are built on 8 host threads: construction runs on its own stream with
             # stream-ordered buffers, so builds overlap one another on the GPU.
+            t0 = time.perf_counter()
             fresh = list(builders.map(lambda s: api.Scene(s, split_references=True), snaps))
+            t1 = time.perf_counter()
             batch = [api.BatchJob(f, j.render, j.integrator) for f, j in zip(fresh, jobs)]
             _, codes, _ = api.render_batch(batch, tuned)
             assert all(c == 0 for c in codes), codes
+            phase["build"] += t1 - t0
+            phase["render"] += time.perf_counter() - t1
             for f in fresh:
                 f.close()
 
         e2e_step()
         barrier()
         torch.cuda.synchronize()
+        phase = {"build": 0.0, "render": 0.0}
         w0 = time.perf_counter()
         for _ in range(args.steps):
             e2e_step()
@@ -541,6 +548,7 @@ def run_ours(args):
         if world > 1:
             dist.all_reduce(e2e_seconds, op=dist.ReduceOp.MAX)
         e2e_value = world * samples * args.steps / float(e2e_seconds.item()) / 1e6
+        e2e_phase = phase
 
     serving = sustainable = None
     if world == 1 and not args.no_serve:
@@ -622,7 +630,9 @@ def run_ours(args):
                     "d2h_bytes_per_step": d2h,
                     "step": "256 scene uploads from pinned memory + GPU BVH builds (8 host "
                             "threads) + batched render + image read-back "
-                            "(mr_scene_create_with + mr_render_batch)"},
+                            "(mr_scene_create_with + mr_render_batch)",
+                    "scene_build_s_per_step": e2e_phase["build"] / args.steps if e2e_phase else None,
+                    "render_s_per_step": e2e_phase["render"] / args.steps if e2e_phase else None},
             "gpu_launches": launches,
             "clocks": clock_info,
         }

@@ -507,8 +507,9 @@ mr_status mr_render_batch(mr_batch_job* jobs, size_t count, const mr_batch_setti
                           mr_batch_statistics* statistics);
 
 /* Autotuner: renders the calibration jobs once per candidate wave shape (paths per wave,
- * resident blocks, sort threshold), keeps the fastest and writes it to `best` together with the
- * samples/s it reached. Images are not copied back. */
+ * concurrent waves, sort threshold), then renders the three fastest shapes, each also with fewer
+ * resident traversal blocks, twice more; writes the shape of the best run to `best` together with
+ * the samples/s (per device second) it reached. Images are not copied back. */
 mr_status mr_batch_autotune(const mr_batch_job* jobs, size_t count, mr_batch_settings* best,
                             double* samples_per_second);
 

@@ -15,7 +15,10 @@
 
 namespace mr {
 
-constexpr int      kStackSize  = 145;  // a wide node pushes <= 3 entries; <= 48 levels (bvh.cpp:126)
+// A wide node pushes <= 3 entries and sits at most 63 levels deep (built trees stop at 48,
+// bvh.cpp:126; imported trees are refused beyond 64 levels), so at most 3 * 63 entries are
+// stacked before any push: the check `sp > kStackSize - 3` never fires on an accepted tree.
+constexpr int      kStackSize  = 195;
 constexpr uint32_t kMaxVisits  = 1u << 16;  // node visits per ray before the query gives up
 
 struct RayQuery {
@@ -247,8 +250,7 @@ __device__ __forceinline__ TraceResult trace(const DeviceScene& s, const RayQuer
             order2(t1, r1, t3, r3);
             order2(t1, r1, t2, r2);
             if (t0 != inf) {
-                const int pushes = (t1 != inf) + (t2 != inf) + (t3 != inf);
-                if (sp + pushes > kStackSize) {
+                if (sp > kStackSize - 3) {
                     error |= kErrorStack;
                     return result;
                 }
