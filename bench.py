@@ -106,17 +106,24 @@ def trace_sample(k):
     lib.mr_set_kernel_timing(0)
     algorithmic = (BYTES_PER_BOUNDS_TEST * counted.bounds_tests +
                    BYTES_PER_TRIANGLE_TEST * counted.triangle_tests)
-    # Rays traced: camera rays, an extension ray per scattering event that survived roulette,
-    # shadow rays.
-    rays = (stats["paths"] + stats["scattering_events"] - stats["roulette_terminations"] +
-            stats["shadow_rays"])
+    kinds = ray_counts(stats)
+    rays = sum(kinds.values())
     print(json.dumps({"job": k, **job, "trace_launches": launches.value,
-                      "rays": rays, "rays_per_second": rays / seconds.value,
+                      "rays": rays, "rays_by_kind": kinds,
+                      "rays_per_second": rays / seconds.value,
                       "bounds_tests": counted.bounds_tests,
                       "triangle_tests": counted.triangle_tests,
                       "algorithmic_bytes": algorithmic, "trace_seconds": seconds.value,
                       "all_launches": all_launches.value}), flush=True)
     return 0
+
+
+def ray_counts(paths):
+    """Rays traced, by kind, from path statistics: a camera ray per path, an extension ray per
+    scattering event that survived roulette, and the shadow rays."""
+    return {"primary": paths["paths"],
+            "extension": paths["scattering_events"] - paths["roulette_terminations"],
+            "shadow": paths["shadow_rays"]}
 
 
 def rank_info():
@@ -435,11 +442,14 @@ def run_ours(args):
     clocks.start()
     device_seconds, wall0 = 0.0, time.perf_counter()
     launches, waves = 0, 0
+    rays = {"primary": 0, "extension": 0, "shadow": 0}
     for _ in range(args.steps):
         info = step()
         device_seconds += info["device_seconds"]
         launches += info["kernel_launches"]
         waves += info["waves"]
+        for kind, n in ray_counts(info["paths"]).items():
+            rays[kind] += n
     torch.cuda.synchronize()
     wall = time.perf_counter() - wall0
     barrier()
@@ -610,6 +620,11 @@ def run_ours(args):
                                      "tuning_s": tune_seconds},
                        "wall_ms_per_step": 1e3 * wall / args.steps,
                        "waves_per_step": waves / args.steps,
+                       "rays": {"per_step": {kind: n // args.steps for kind, n in rays.items()},
+                                "Grays_per_s": world * sum(rays.values()) / worst / 1e9,
+                                "counted": "primary = camera paths, extension = scattering "
+                                           "events that survived roulette, shadow = shadow "
+                                           "rays (engine path statistics)"},
                        "scene_generation_s": gen_seconds, "scene_build_s": scene_seconds,
                        "plain_gpu": {"value": plain_value, "unit": METRIC,
                                      "ms_per_step": 1e3 * plain_seconds,
