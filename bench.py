@@ -54,6 +54,9 @@ TABLE_SEED = 3
 FALLBACK_HBM_GBS = 6650.0
 BYTES_PER_BOUNDS_TEST = 24   # one FP32 AABB
 BYTES_PER_TRIANGLE_TEST = 36  # one FP32 triangle
+FLOPS_PER_BOUNDS_TEST = 24    # ~12 FP32 FMA-equivalents: six plane distances, min/max
+FLOPS_PER_TRIANGLE_TEST = 80  # ~40 FP32 FMA-equivalents: shear, edge functions, error bound
+SM_MAX_MHZ = 1965.0           # B200 maximum SM clock, when nvidia-smi reports none
 CPU_SAMPLE_JOBS = (0, 64, 128, 192)
 SERVE_RATE = 50.0             # jobs per second (the serving workload)
 SUSTAINABLE_RATE = 16.0       # jobs per second that one B200 keeps up with on this job mix
@@ -593,6 +596,13 @@ def run_ours(args):
                    BYTES_PER_TRIANGLE_TEST * counted.triangle_tests)
     achieved = algorithmic / ksec.value / 1e9 if ksec.value > 0 else 0.0
     per_launch = algorithmic / max(1, k_launches.value)
+    # The arithmetic side of the same launches: FP32 operations (FMA-equivalents counted as two
+    # flops) per test, against the nominal FP32 rate of the CUDA cores (128 lanes per SM).
+    flops = FLOPS_PER_BOUNDS_TEST * counted.bounds_tests + FLOPS_PER_TRIANGLE_TEST * counted.triangle_tests
+    props = torch.cuda.get_device_properties(local)
+    max_mhz = (clock_info or {}).get("sm_max_mhz") or SM_MAX_MHZ
+    fp32_peak = props.multi_processor_count * 128 * 2 * max_mhz * 1e6 / 1e12
+    flops_achieved = flops / ksec.value / 1e12 if ksec.value > 0 else 0.0
     traffic = None
     tfile = os.path.join(ROOT, "profiles", "trace_kernel_traffic.txt")
     if os.path.exists(tfile):
@@ -640,7 +650,11 @@ def run_ours(args):
                          "algorithmic_bytes_per_launch": per_launch,
                          "launches": k_launches.value,
                          "avg_launch_ms": 1e3 * ksec.value / max(1, k_launches.value),
-                         "bytes_model": "24 B per bounds test + 36 B per triangle test"},
+                         "bytes_model": "24 B per bounds test + 36 B per triangle test",
+                         "fp32": {"achieved": flops_achieved, "peak": fp32_peak,
+                                  "unit": "TFLOP/s", "frac": flops_achieved / fp32_peak,
+                                  "peak_source": "nominal: SMs x 128 FP32 lanes x 2 x max SM clock",
+                                  "flops_model": "24 per bounds test + 80 per triangle test"}},
             "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h,
                     "step": "256 scene uploads from pinned memory + GPU BVH builds (8 host "
