@@ -507,6 +507,33 @@ def run_ours(args):
                   "plain": small_samples / small_plain / 1e6,
                   "batched_vs_plain": small_plain / small_batched, "unit": METRIC}
 
+    # Preview-sized renders of the same scenes (128x128, 4 spp, each job's depth): the regime in
+    # which one launch sequence per job leaves most of the GPU idle.
+    tiny = [api.BatchJob(j.scene, api.RenderSettings(128, 128, 4, j.render.seed), j.integrator)
+            for j in jobs]
+    tiny_samples = sum(j.render.width * j.render.height * j.render.samples_per_pixel for j in tiny)
+    try:
+        api.render_batch(tiny, tuned, copy_images=False)  # warm-up
+        _, codes, info = api.render_batch(tiny, tuned, copy_images=False)
+        assert all(c == 0 for c in codes), codes
+        tiny_batched = info["device_seconds"]
+        for j in tiny[:4]:
+            api.PathTracer(j.scene, j.integrator).render_device(j.render, image.data_ptr(),
+                                                                stream.cuda_stream)
+        e0.record(stream)
+        for j in tiny:
+            api.PathTracer(j.scene, j.integrator).render_device(j.render, image.data_ptr(),
+                                                                stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        tiny_plain = e0.elapsed_time(e1) / 1e3
+        tiny_jobs = {"jobs": len(tiny), "samples": tiny_samples, "render": "128x128, 4 spp",
+                     "batched": tiny_samples / tiny_batched / 1e6,
+                     "plain": tiny_samples / tiny_plain / 1e6,
+                     "batched_vs_plain": tiny_plain / tiny_batched, "unit": METRIC}
+    except Exception as error:  # a secondary leg: report it, keep the line
+        tiny_jobs = {"error": f"{type(error).__name__}: {error}"}
+
     # The single 1M-triangle frame (plain path), after one warm-up frame.
     large = api.Scene(sc.large_scene().snapshot())
     frame_render = api.RenderSettings(1920, 1080, 64, 1 + rank)
@@ -641,6 +668,7 @@ def run_ours(args):
                                      "engine": "mr_render_device, one job per call"},
                        "batched_vs_plain": value / plain_value,
                        "small_jobs": small_jobs,
+                       "preview_jobs": tiny_jobs,
                        "serving": serving, "serving_sustainable": sustainable,
                        "large_frame": large_frame, "stress": stress},
             "roofline": {"bound": "hbm", "kernel": "trace_kernel (nearest-hit + shadow "

@@ -38,3 +38,6 @@ def test_bench_prints_the_contract_line():
     assert rays["primary"] == samples  # one camera ray per sample
     assert rays["extension"] > 0 and rays["shadow"] > 0
     assert {"sm_mhz", "sm_max_mhz", "reasons"} <= set(line["clocks"])
+    preview = line["config"]["preview_jobs"]
+    assert "error" not in preview, preview
+    assert preview["batched"] > 0 and preview["plain"] > 0
