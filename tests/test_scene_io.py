@@ -160,17 +160,3 @@ def test_reference_scene_files_load(oracle):
     image, stats = oracle.OracleScene(doc.snapshot(), oracle.integrator("mis", 4, True, 3)).render(
         _abi.RenderSettings(16, 12, 2, 1), threads=2)
     assert np.isfinite(image).all() and image.mean() > 0 and stats["paths"] == 16 * 12 * 2
-
-
-@pytest.mark.parametrize("args,message", [
-    (["s.json"], "Usage"),
-    (["s.json", "out", "--integrator", "sppm"], "SPPM"),
-    (["s.json", "out", "--bogus", "1"], "Unknown render option"),
-    (["s.json", "out", "--width"], "missing its value"),
-    (["s.json", "out", "--mode", "fast"], "Sampling mode"),
-    (["s.json", "out", "--exposure", "100"], "Exposure"),
-])
-def test_render_command_rejects_bad_options(args, message):
-    from minirender_b200 import render_cli
-    with pytest.raises(ValueError, match=message):
-        render_cli.run(args)
