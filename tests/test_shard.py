@@ -105,3 +105,74 @@ def test_two_gloo_ranks_gather_frame_and_jobs(oracle):
                                   np.load(os.path.join(out, f"job{k}_ref.npy")))
         counts = [int(np.load(os.path.join(out, f"count{r}.npy"))[0]) for r in range(2)]
         assert sum(counts) == 7 and min(counts) >= 1
+
+
+def test_partition_with_more_ranks_than_jobs():
+    assert shard.partition_jobs([], 4) == [[], [], [], []]
+    shares = shard.partition_jobs([5, 9, 1], 8)
+    assert sorted(i for s in shares for i in s) == [0, 1, 2]
+    assert sum(1 for s in shares if s) == 3 and all(len(s) <= 1 for s in shares)
+
+
+def _worker_sparse(rank, world, port, out):
+    # Three ranks, a two-row frame and two jobs: rank 2 holds an empty row band and no job.
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=120))
+    from minirender_b200 import api, scene as sc
+    from oracle import pyoracle
+    try:
+        doc = sc.cornell_box()
+        o = pyoracle.OracleScene(doc.snapshot(), pyoracle.integrator("mis", 3, True, 3))
+        render = api.RenderSettings(6, 2, 2, 9)
+        seen = []
+
+        def band(r, begin, end):
+            seen.append((begin, end))
+            img, _ = o.render(r.c(), threads=1, rows=(begin, end), statistics=False)
+            return np.asarray(img)[: end - begin].reshape(end - begin, r.width, 3)
+
+        frame = shard.render_frame_sharded(None, render, band_renderer=band)
+
+        class Job:
+            def __init__(self, k):
+                self.render = api.RenderSettings(4 + k, 3, 1, 21 + k)
+                self.integrator = api.IntegratorSettings("mis", 3, True, 3)
+
+        def alone(job):
+            return o.render(job.render.c(), threads=1, statistics=False)[0]
+
+        jobs = [Job(0), Job(1)]
+        rendered = []
+
+        def batch(share):
+            rendered.extend(share)
+            return [alone(j) for j in share]
+
+        images = shard.render_jobs_sharded(jobs, batch_renderer=batch)
+        np.save(os.path.join(out, f"sparse{rank}.npy"), np.array([len(rendered), *seen[0]]))
+        if rank == 0:
+            np.save(os.path.join(out, "sparse_frame.npy"), frame)
+            np.save(os.path.join(out, "sparse_frame_ref.npy"),
+                    o.render(render.c(), threads=1, statistics=False)[0])
+            for k, (job, image) in enumerate(zip(jobs, images)):
+                np.save(os.path.join(out, f"sparse_job{k}.npy"), image)
+                np.save(os.path.join(out, f"sparse_job{k}_ref.npy"), alone(job))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_three_gloo_ranks_with_an_empty_band_and_no_job(oracle):
+    import torch.multiprocessing as mp
+    with tempfile.TemporaryDirectory() as out:
+        mp.start_processes(_worker_sparse, args=(3, _free_port(), out), nprocs=3, join=True,
+                           start_method="spawn")
+        assert np.array_equal(np.load(os.path.join(out, "sparse_frame.npy")),
+                              np.load(os.path.join(out, "sparse_frame_ref.npy")))
+        for k in range(2):
+            assert np.array_equal(np.load(os.path.join(out, f"sparse_job{k}.npy")),
+                                  np.load(os.path.join(out, f"sparse_job{k}_ref.npy")))
+        info = [np.load(os.path.join(out, f"sparse{r}.npy")) for r in range(3)]
+        assert [int(i[0]) for i in info] == [1, 1, 0]  # jobs per rank (LPT: larger job first)
+        assert [tuple(int(v) for v in i[1:]) for i in info] == [(0, 1), (1, 2), (2, 2)]
