@@ -420,8 +420,9 @@ def render_batch(jobs: list[BatchJob], settings: BatchSettings | None = None,
 
 
 def autotune(jobs: list[BatchJob]):
-    """Runs the calibration jobs once per candidate wave shape and returns the fastest
-    (BatchSettings, samples per second)."""
+    """Runs the calibration jobs once per candidate wave shape, then the three fastest shapes
+    (each also with fewer resident traversal blocks) twice more, and returns the best run's
+    (BatchSettings, samples per device second)."""
     lib = load_library()
     records = _batch_records(jobs, None)
     best = _abi.BatchSettings()
