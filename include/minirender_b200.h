@@ -378,10 +378,13 @@ mr_status mr_capture_shadow_rays(const mr_scene* scene, const mr_integrator_sett
  * (seed, pixel, sample per path) and `device_radiance` (3 floats per path) are device memory;
  * `stream` is a cudaStream_t (null = legacy default stream); the call returns after the work
  * has finished. The working memory is one fixed array of about 4.2 MB inside the library, held
- * on every GPU that loads it until the process exits; the first call on a device looks up its
- * address and should come before any stream capture. Calls share that array: it is cleared at
- * the start of each call, and calls whose GPU work overlaps race. Larger batches are rejected
- * with MR_INVALID_ARGUMENT. */
+ * on every GPU that loads it until the process exits. The first call on a device looks up the
+ * array's address, which under CUDA's lazy module loading also loads the module and places the
+ * array in device memory (an allocation and a synchronisation): warm up each device with a call
+ * of count 0 (null buffers allowed) before any stream capture and before the phase that must not
+ * allocate. The address is cached per device and must not be used across a cudaDeviceReset.
+ * Calls share that array: it is cleared at the start of each call, and calls whose GPU work
+ * overlaps race. Larger batches are rejected with MR_INVALID_ARGUMENT. */
 mr_status mr_trace_paths_static(const mr_scene* scene, const mr_integrator_settings* integrator,
                                 const mr_ray* device_rays, const uint64_t* device_keys,
                                 size_t count, float* device_radiance, void* stream);

@@ -10,15 +10,20 @@
 // process exits). Inputs and outputs stay in the caller's device memory.
 //
 // The array's device address is resolved once per device with cudaGetSymbolAddress (the name in
-// host code is only a host-side stand-in); the first call on a device does this and should
-// therefore come before any stream capture. Every call reuses the same array, which keeps the
-// previous call's contents: counters, statistics and error words are cleared at the start of
-// each call, and calls whose GPU work overlaps (several streams or threads at once) race on it.
+// host code is only a host-side stand-in). The first call on a device does this, and with CUDA's
+// lazy module loading that lookup is also what loads the module and places the array in device
+// memory (which can allocate and synchronise): make that first call a zero-length one (count 0),
+// before any stream capture and before the caller's no-allocation phase. The cached address
+// belongs to the device's primary context: the entry point must not be used across a
+// cudaDeviceReset of that device. Every call reuses the same array, which keeps the previous
+// call's contents: counters, statistics and error words are cleared at the start of each call,
+// and calls whose GPU work overlaps (several streams or threads at once) race on it.
 #include <array>
 #include <cmath>
 #include <mutex>
 
 #include "errors.hpp"
+#include "validation.hpp"
 #include "wavefront.cuh"
 
 struct mr_scene {
@@ -107,7 +112,9 @@ void carve(unsigned char* base, Workspace& ws, float4*& staging, unsigned*& inva
 }
 
 // RayQuery / RayInterval validation (src/render/intersection.cpp:22-26,123-130) on the device,
-// plus the copy into the wave's ray records.
+// plus the copy into the wave's ray records. The unit-length check evaluates the squared length
+// in FP64 with the host check's operation order (validate_ray in abi.cu), so this entry point
+// rejects exactly the rays mr_trace_paths rejects; no path arithmetic uses FP64.
 __global__ void stage_rays_kernel(const mr_ray* rays, uint32_t count, float4* staging,
                                   unsigned* invalid) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -119,9 +126,9 @@ __global__ void stage_rays_kernel(const mr_ray* rays, uint32_t count, float4* st
     for (int a = 0; a < 3; ++a) {
         ok = ok && isfinite(r.origin[a]) && isfinite(r.direction[a]);
     }
-    const float d2 = (r.direction[0] * r.direction[0] + r.direction[1] * r.direction[1]) +
-                     r.direction[2] * r.direction[2];
-    ok = ok && fabsf(d2 - 1.0f) <= 1e-4f && isfinite(r.minimum) && r.minimum >= 0 &&
+    const double x = r.direction[0], y = r.direction[1], z = r.direction[2];
+    const double d2 = __dadd_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), __dmul_rn(z, z));
+    ok = ok && fabs(d2 - 1.0) <= 1e-4 && isfinite(r.minimum) && r.minimum >= 0 &&
          !isnan(r.maximum) && r.maximum >= r.minimum;
     if (!ok) {
         atomicOr(invalid, 1u);
@@ -152,24 +159,18 @@ extern "C" mr_status mr_trace_paths_static(const mr_scene* scene,
                                            size_t count, float* device_radiance, void* stream) {
     try {
         require(scene != nullptr && scene->impl != nullptr, "Scene handle is null");
-        IntegratorParams p{MR_SAMPLING_MIS, 8, 1, 3};
-        if (integrator) {
-            p = {integrator->mode, integrator->maximum_depth, integrator->russian_roulette ? 1u : 0u,
-                 integrator->roulette_depth};
-        }
-        require(p.mode <= MR_SAMPLING_MIS, "Sampling mode must be bsdf, light or mis");
-        require(p.maximum_depth <= 128 && p.roulette_depth <= 128,
-                "Path and roulette depths must not exceed 128");
+        const IntegratorParams p = integrator_params(integrator);
         if (count > kStaticPaths) {
             fail(MR_INVALID_ARGUMENT,
                  "mr_trace_paths_static takes at most MR_STATIC_MAX_PATHS (16384) paths per call");
         }
+        // Resolved before the zero-length return, so a call with count 0 is the warm-up.
+        unsigned char* base = device_scratch();
         if (count == 0) {
             return MR_OK;
         }
         require(device_rays && device_keys && device_radiance, "Path buffers are null");
         cudaStream_t   s    = static_cast<cudaStream_t>(stream);
-        unsigned char* base = device_scratch();
         Workspace      ws;
         float4*        staging = nullptr;
         unsigned*      invalid = nullptr;

@@ -20,6 +20,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <exception>
 #include <limits>
 #include <map>
 #include <memory>
@@ -2064,6 +2065,41 @@ struct DRay {
 
 }  // namespace
 
+namespace {
+
+// Splits [0, count) into contiguous chunks over the host's threads (one chunk below 65,536
+// items); every chunk gets its own statistics, summed after the join.
+template <typename F>
+void parallel_chunks(size_t count, oracle::TraceStatistics& total, F&& body) {
+    const size_t threads = count < 65536 ? 1 : std::max(1U, std::thread::hardware_concurrency());
+    std::vector<oracle::TraceStatistics> local(threads);
+    std::vector<std::exception_ptr>      errors(threads);
+    const auto run = [&](size_t t) {
+        try {
+            body(count * t / threads, count * (t + 1) / threads, local[t]);
+        } catch (...) {
+            errors[t] = std::current_exception();
+        }
+    };
+    std::vector<std::thread> pool;
+    for (size_t t = 1; t < threads; ++t) {
+        pool.emplace_back(run, t);
+    }
+    run(0);
+    for (auto& t : pool) {
+        t.join();
+    }
+    for (size_t t = 0; t < threads; ++t) {
+        if (errors[t]) {
+            std::rethrow_exception(errors[t]);
+        }
+        total.bounds_tests += local[t].bounds_tests;
+        total.triangle_tests += local[t].triangle_tests;
+    }
+}
+
+}  // namespace
+
 extern "C" {
 
 size_t or_last_error(char* buffer, size_t capacity) {
@@ -2272,25 +2308,28 @@ int or_intersect(void* scene, const DRay* rays, size_t count, double* hits, uint
     return guarded([&] {
         const auto&             bvh = static_cast<OracleScene*>(scene)->tracer->bvh();
         oracle::TraceStatistics stats;
-        for (size_t i = 0; i < count; ++i) {
-            const auto& r = rays[i];
-            const oracle::Ray ray{{r.origin[0], r.origin[1], r.origin[2]},
-                                  {r.direction[0], r.direction[1], r.direction[2]}};
-            const auto hit = bvh.intersect(ray, {r.minimum, r.maximum}, &stats);
-            double*    o   = hits + 18 * i;
-            std::memset(o, 0, sizeof(double) * 18);
-            if (hit) {
-                o[0] = 1, o[1] = hit->distance, o[2] = hit->instance_index, o[3] = hit->triangle_index;
-                o[4] = hit->primitive;
-                o[5] = hit->barycentric.x, o[6] = hit->barycentric.y, o[7] = hit->barycentric.z;
-                o[8] = hit->front_face;
-                o[9] = hit->position.x, o[10] = hit->position.y, o[11] = hit->position.z;
-                o[12] = hit->geometric_normal.x, o[13] = hit->geometric_normal.y,
-                o[14] = hit->geometric_normal.z;
-                o[15] = hit->shading_normal.x, o[16] = hit->shading_normal.y,
-                o[17] = hit->shading_normal.z;
+        parallel_chunks(count, stats, [&](size_t begin, size_t end, oracle::TraceStatistics& st) {
+            for (size_t i = begin; i < end; ++i) {
+                const auto& r = rays[i];
+                const oracle::Ray ray{{r.origin[0], r.origin[1], r.origin[2]},
+                                      {r.direction[0], r.direction[1], r.direction[2]}};
+                const auto hit = bvh.intersect(ray, {r.minimum, r.maximum}, &st);
+                double*    o   = hits + 18 * i;
+                std::memset(o, 0, sizeof(double) * 18);
+                if (hit) {
+                    o[0] = 1, o[1] = hit->distance, o[2] = hit->instance_index,
+                    o[3] = hit->triangle_index;
+                    o[4] = hit->primitive;
+                    o[5] = hit->barycentric.x, o[6] = hit->barycentric.y, o[7] = hit->barycentric.z;
+                    o[8] = hit->front_face;
+                    o[9] = hit->position.x, o[10] = hit->position.y, o[11] = hit->position.z;
+                    o[12] = hit->geometric_normal.x, o[13] = hit->geometric_normal.y,
+                    o[14] = hit->geometric_normal.z;
+                    o[15] = hit->shading_normal.x, o[16] = hit->shading_normal.y,
+                    o[17] = hit->shading_normal.z;
+                }
             }
-        }
+        });
         if (counters) {
             counters[0] += stats.bounds_tests;
             counters[1] += stats.triangle_tests;
@@ -2302,12 +2341,14 @@ int or_occluded(void* scene, const DRay* rays, size_t count, uint8_t* out, uint6
     return guarded([&] {
         const auto&             bvh = static_cast<OracleScene*>(scene)->tracer->bvh();
         oracle::TraceStatistics stats;
-        for (size_t i = 0; i < count; ++i) {
-            const auto&       r = rays[i];
-            const oracle::Ray ray{{r.origin[0], r.origin[1], r.origin[2]},
-                                  {r.direction[0], r.direction[1], r.direction[2]}};
-            out[i] = bvh.occluded(ray, {r.minimum, r.maximum}, &stats) ? 1 : 0;
-        }
+        parallel_chunks(count, stats, [&](size_t begin, size_t end, oracle::TraceStatistics& st) {
+            for (size_t i = begin; i < end; ++i) {
+                const auto&       r = rays[i];
+                const oracle::Ray ray{{r.origin[0], r.origin[1], r.origin[2]},
+                                      {r.direction[0], r.direction[1], r.direction[2]}};
+                out[i] = bvh.occluded(ray, {r.minimum, r.maximum}, &st) ? 1 : 0;
+            }
+        });
         if (counters) {
             counters[0] += stats.bounds_tests;
             counters[1] += stats.triangle_tests;
@@ -2361,6 +2402,27 @@ int or_sample_pixels(void* scene, const mr_render_settings* render, const uint32
             }
         }
         to_path_stats(stats, statistics);
+    });
+}
+
+// Pinhole camera rays at explicit film coordinates with the clip interval of the primary-ray
+// diagnostic (src/app/cli.cpp:60-81: Camera::generate_ray at the pixel centre, interval
+// near/cos .. far/cos with cos the ray's cosine to the view direction).
+int or_camera_rays(void* scene, const double* uv, size_t count, double aspect, DRay* rays) {
+    return guarded([&] {
+        const auto& tracer  = *static_cast<OracleScene*>(scene)->tracer;
+        const auto& camera  = tracer.scene().camera;
+        const auto  forward = oracle::normalize(oracle::from(camera.target) - oracle::from(camera.position));
+        for (size_t i = 0; i < count; ++i) {
+            const auto   ray    = tracer.generate_ray({uv[2 * i], uv[2 * i + 1]}, aspect);
+            const double cosine = oracle::dot(ray.direction, forward);
+            for (int a = 0; a < 3; ++a) {
+                rays[i].origin[a]    = ray.origin[a];
+                rays[i].direction[a] = ray.direction[a];
+            }
+            rays[i].minimum = camera.near_plane / cosine;
+            rays[i].maximum = camera.far_plane / cosine;
+        }
     });
 }
 

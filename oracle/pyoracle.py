@@ -36,9 +36,13 @@ _lib = None
 
 
 def lib():
+    """The oracle library: liboracle.so (nofma without hardware FMA), or the variant the
+    environment names in ORACLE_VARIANT ("contract": multiply-adds fused by the compiler)."""
     global _lib
     if _lib is None:
         name = "liboracle.so" if _cpu_has_fma() else "liboracle_nofma.so"
+        if os.environ.get("ORACLE_VARIANT") == "contract":
+            name = "liboracle_contract.so"
         path = os.path.join(BUILD, name)
         if not os.path.exists(path):
             build()
@@ -87,6 +91,7 @@ def _declare(l):
         "or_sample_pixels": (C.c_int, [VP, P(_abi.RenderSettings), P(C.c_uint32),
                                        P(C.c_uint64), C.c_size_t, dp, P(DRay),
                                        P(_abi.PathStatistics)]),
+        "or_camera_rays": (C.c_int, [VP, dp, C.c_size_t, C.c_double, P(DRay)]),
         "or_render_rows": (C.c_int, [VP, P(_abi.RenderSettings), C.c_uint64, C.c_uint64,
                                      C.c_uint32, P(C.c_float), P(_abi.PathStatistics)]),
         "or_light_sample": (C.c_int, [VP, dp, C.c_double, dp, dp]),
@@ -349,6 +354,15 @@ class OracleScene:
             r = np.frombuffer(rays, dtype=np.float64).reshape(-1, 8)[:n].copy()
             return out[:n], stats.as_dict(), r
         return out[:n], stats.as_dict()
+
+    def camera_rays(self, uv, aspect):
+        """Pinhole rays at film coordinates `uv` (n, 2) with the primary-ray diagnostic's clip
+        interval: (n, 8) [origin, direction, minimum, maximum]."""
+        uv = np.ascontiguousarray(uv, np.float64).reshape(-1, 2)
+        n = len(uv)
+        rays = (DRay * max(1, n))()
+        _check(lib().or_camera_rays(self.handle, _ptr(uv, C.c_double), n, aspect, rays))
+        return np.frombuffer(rays, dtype=np.float64).reshape(-1, 8)[:n].copy()
 
     def render(self, render, threads=None, rows=None, statistics=True):
         threads = threads or max(1, os.cpu_count() or 1)

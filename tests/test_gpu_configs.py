@@ -1,0 +1,205 @@
+"""Parity at the benchmark configurations' own sizes, GPU (through the C ABI) against the FP64
+oracle with the oracle's reference-algorithm BVH imported:
+
+  * config 1: the 36-triangle Cornell box at 512x512, 16 spp, depth 8, Russian roulette from
+    depth 3, MIS, seeds 1, 2 and 3 (PathTracer::render, src/render/path_tracer.cpp:388-405);
+  * config 2: a 16-row band through the middle of the 1920x1080, 64 spp, depth 12 frame of the
+    1.02M-triangle scene (thin lens, diffuse/GGX/mirror/glass, constant environment and a
+    directional light).
+
+Bars:
+  * hit records, for every camera ray of the frame (config 1) or band (config 2) and for the
+    first shadow ray of every such path: equal hit/miss and primitive id except the classes of
+    tests/hit_classes.py (ties within 1 FP32 ulp, edge grazes within the FP32 edge-function error
+    bound, interval ends), none unexplained, and those classes together in at most 1 of 20,000
+    rays;
+  * images: a pixel agrees when every channel has |gpu - cpu| <= 1e-3 * max(cpu, 0.05 * mean).
+    A pixel that does not must be explained by divergent samples: its samples are traced again
+    one by one on both sides, and at least one must differ by more than the same tolerance (its
+    path took another discrete decision: a roulette, light-selection or lobe choice, or a hit
+    record of the classes above, decided differently in FP32). Divergent samples found this way
+    are at most 1 in 20,000 samples; image means agree within 0.1% and the path counters (shadow
+    rays, scattering events, roulette terminations) within 1e-4 relative;
+  * the GPU binned-SAH builder's tree of the 1.02M-triangle scene costs within 2% of the
+    reference builder's.
+"""
+
+import numpy as np
+import pytest
+
+from minirender_b200 import scene as sc
+from tests import hit_classes
+
+pytestmark = pytest.mark.gpu
+
+PIXEL_TOL = 1e-3
+RATE = 20_000  # at most one classified hit-record difference / divergent sample per RATE
+
+
+@pytest.fixture(scope="module")
+def api():
+    from minirender_b200 import api as a
+    return a
+
+
+@pytest.fixture(scope="module")
+def cornell(api, oracle):
+    snap = sc.cornell_box().snapshot()
+    o = oracle.OracleScene(snap, oracle.integrator("mis", 8, True, 3))
+    return api.Scene(snap, o.export_bvh()), o
+
+
+@pytest.fixture(scope="module")
+def large(api, oracle):
+    snap = sc.large_scene().snapshot()
+    o = oracle.OracleScene(snap, oracle.integrator("mis", 12, True, 3))
+    return api.Scene(snap, o.export_bvh()), o, snap
+
+
+def pixel_grid(width, rows, spp):
+    ys, xs = np.meshgrid(np.arange(rows[0], rows[1]), np.arange(width), indexing="ij")
+    pixels = np.repeat(np.stack([xs.ravel(), ys.ravel()], 1), spp, axis=0).astype(np.uint32)
+    samples = np.tile(np.arange(spp, dtype=np.uint64), xs.size)
+    return pixels, samples
+
+
+def check_camera_hits(api, g, o, render, settings, rows):
+    pixels, samples = pixel_grid(render.width, rows, render.samples_per_pixel)
+    tracer = api.PathTracer(g, settings)
+    _, _, rays = tracer.sample_pixels(render, pixels, samples, want_rays=True)
+    g_hits, _ = g.intersect(rays[:, 0:3], rays[:, 3:6], rays[:, 6], rays[:, 7])
+    c_hits, _ = o.intersect(rays[:, 0:3], rays[:, 3:6], rays[:, 6], rays[:, 7])
+    classes, bad = hit_classes.compare_nearest(
+        g_hits["primitive"], c_hits[:, 0] == 1, c_hits[:, 4], o.primitives(), rays[:, 0:3],
+        rays[:, 3:6], rays[:, 6], rays[:, 7])
+    assert classes["unexplained"] == 0, (classes, bad)
+    assert classes["tie"] + classes["graze"] + classes["interval"] <= len(rays) // RATE, classes
+    return classes, len(rays)
+
+
+def check_shadow_hits(api, g, o, render, settings, rows):
+    pixels, samples = pixel_grid(render.width, rows, render.samples_per_pixel)
+    tracer = api.PathTracer(g, settings)
+    rays, has, occ = tracer.capture_shadow_rays(render, pixels, samples)
+    r = rays[has]
+    g_occ = occ[has]
+    c_occ, _ = o.occluded(r[:, 0:3], r[:, 3:6], r[:, 6], r[:, 7])
+    differ = np.flatnonzero(g_occ != c_occ)
+    # The occluder that decided each difference: the nearest primitive each side finds in the
+    # same segment.
+    g_near, _ = g.intersect(r[differ, 0:3], r[differ, 3:6], r[differ, 6], r[differ, 7])
+    c_near, _ = o.intersect(r[differ, 0:3], r[differ, 3:6], r[differ, 6], r[differ, 7])
+    where = {int(i): k for k, i in enumerate(differ)}
+
+    def g_prim(i):
+        p = g_near["primitive"][where[int(i)]]
+        return None if p == 0xFFFFFFFF else int(p)
+
+    def c_prim(i):
+        k = where[int(i)]
+        return int(c_near[k, 4]) if c_near[k, 0] == 1 else None
+
+    classes, bad = hit_classes.compare_occlusion(g_occ, c_occ, g_prim, c_prim, o.primitives(),
+                                                 r[:, 0:3], r[:, 3:6], r[:, 6], r[:, 7])
+    assert classes["unexplained"] == 0, (classes, bad)
+    assert classes["tie"] + classes["graze"] + classes["interval"] <= max(1, len(r) // RATE), classes
+    return classes, len(r)
+
+
+def check_image(api, g, o, render, settings, rows):
+    tracer = api.PathTracer(g, settings)
+    if rows == (0, render.height):
+        gpu, gstats = tracer.render(render)
+    else:
+        gpu, gstats = tracer.render_rows(render, rows[0], rows[1], statistics=True)
+    cpu, cstats = o.render(render.c(), rows=rows)
+    mean = float(cpu.mean())
+    scale = np.maximum(cpu, 0.05 * mean)
+    bad = np.flatnonzero(~np.all(np.abs(gpu - cpu) <= PIXEL_TOL * scale, axis=2).ravel())
+    # Explain every disagreeing pixel by its divergent samples.
+    spp = render.samples_per_pixel
+    divergent = 0
+    if len(bad):
+        ys, xs = np.divmod(bad, render.width)
+        pixels = np.repeat(np.stack([xs, ys + rows[0]], 1), spp, axis=0).astype(np.uint32)
+        samples = np.tile(np.arange(spp, dtype=np.uint64), len(bad))
+        gs, _ = tracer.sample_pixels(render, pixels, samples)
+        cs, _ = o.sample_pixels(render.c(), pixels, samples)
+        # The per-sample values are the ones the frame summed.
+        assert np.allclose(gs.reshape(len(bad), spp, 3).mean(1), gpu.reshape(-1, 3)[bad],
+                           rtol=1e-5, atol=1e-7)
+        sample_scale = np.maximum(np.abs(cs), 0.05 * mean)
+        off = ~np.all(np.abs(gs - cs) <= PIXEL_TOL * sample_scale, axis=1)
+        per_pixel = off.reshape(len(bad), spp).sum(1)
+        assert np.all(per_pixel >= 1), (bad[per_pixel == 0][:5], len(bad))
+        divergent = int(off.sum())
+    total = render.width * (rows[1] - rows[0]) * spp
+    assert divergent <= total // RATE, (divergent, len(bad))
+    assert float(gpu.mean()) == pytest.approx(mean, rel=1e-3)
+    assert gstats["paths"] == cstats["paths"] == total
+    for key in ("shadow_rays", "scattering_events", "roulette_terminations"):
+        assert gstats[key] == pytest.approx(cstats[key], rel=1e-4), key
+    return len(bad), divergent
+
+
+# ---- config 1: Cornell box, full frame ----
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_config1_image_matches_oracle(api, cornell, seed):
+    g, o = cornell
+    render = api.RenderSettings(512, 512, 16, seed)
+    bad, divergent = check_image(api, g, o, render, api.IntegratorSettings("mis", 8, True, 3),
+                                 (0, 512))
+    print(f"config 1 seed {seed}: {bad} pixels outside tolerance, {divergent} divergent samples")
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_config1_camera_hit_records(api, cornell, seed):
+    g, o = cornell
+    classes, n = check_camera_hits(api, g, o, api.RenderSettings(512, 512, 16, seed),
+                                   api.IntegratorSettings("mis", 8, True, 3), (0, 512))
+    print(f"config 1 seed {seed}: {n} camera rays, differences {classes}")
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_config1_shadow_hit_records(api, cornell, seed):
+    g, o = cornell
+    classes, n = check_shadow_hits(api, g, o, api.RenderSettings(512, 512, 16, seed),
+                                   api.IntegratorSettings("mis", 8, True, 3), (0, 512))
+    print(f"config 1 seed {seed}: {n} shadow rays, differences {classes}")
+
+
+# ---- config 2: 1.02M triangles, a 16-row band of the 1080p frame ----
+
+BAND = (532, 548)
+
+
+def test_config2_band_image_matches_oracle(api, large):
+    g, o, _ = large
+    render = api.RenderSettings(1920, 1080, 64, 1)
+    bad, divergent = check_image(api, g, o, render, api.IntegratorSettings("mis", 12, True, 3),
+                                 BAND)
+    print(f"config 2 band: {bad} pixels outside tolerance, {divergent} divergent samples")
+
+
+def test_config2_band_camera_hit_records(api, large):
+    g, o, _ = large
+    classes, n = check_camera_hits(api, g, o, api.RenderSettings(1920, 1080, 64, 1),
+                                   api.IntegratorSettings("mis", 12, True, 3), BAND)
+    print(f"config 2 band: {n} camera rays, differences {classes}")
+
+
+def test_config2_band_shadow_hit_records(api, large):
+    g, o, _ = large
+    classes, n = check_shadow_hits(api, g, o, api.RenderSettings(1920, 1080, 64, 1),
+                                   api.IntegratorSettings("mis", 12, True, 3), BAND)
+    print(f"config 2 band: {n} shadow rays, differences {classes}")
+
+
+def test_config2_gpu_builder_sah_within_two_percent(api, large):
+    _, o, snap = large
+    built = api.Scene(snap)
+    assert built.statistics()["triangles"] == snap.triangle_count == 1_024_002
+    assert built.statistics()["maximum_depth"] <= 48
+    assert built.sah_cost() == pytest.approx(o.sah_cost(), rel=0.02)
+    print(f"config 2 SAH: GPU builder {built.sah_cost():.4f}, reference builder {o.sah_cost():.4f}")

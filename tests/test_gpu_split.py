@@ -11,7 +11,7 @@ from minirender_b200 import scene as sc
 
 pytestmark = pytest.mark.gpu
 
-from tests.test_gpu_parity import classify_mismatch  # noqa: E402
+from tests import hit_classes  # noqa: E402
 
 
 @pytest.fixture(scope="module")
@@ -41,8 +41,8 @@ def test_split_tree_gives_identical_hits(api, doc_factory):
     differ = np.nonzero((ha["primitive"] != hb["primitive"]) | (ha["distance"] != hb["distance"]))[0]
     tris = doc.snapshot().world_triangles()
     for i in differ:  # only ties: both triangles at the same FP64 distance
-        cls = classify_mismatch(tris, o[i].astype(np.float64), d[i].astype(np.float64), None,
-                                int(ha["primitive"][i]), int(hb["primitive"][i]))
+        cls = hit_classes.classify(tris, o[i], d[i], 0.0, np.inf, int(ha["primitive"][i]),
+                                   int(hb["primitive"][i]))
         assert cls == "tie", (i, ha[i], hb[i])
     assert len(differ) <= 1e-4 * len(o)
     same = np.setdiff1d(np.arange(len(o)), differ)
