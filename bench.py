@@ -144,13 +144,15 @@ def job_document(job):
     return sc.job_scene(job["triangles"], job["scene_seed"])
 
 
-def config(table, triangles):
+def config(table):
+    """The workload, identical in both arms (the triangle total is what the job scenes build)."""
+    from minirender_b200 import scene as sc
     return {"workload": f"uneven job mix: {len(table)} Cornell rooms with displaced icospheres, "
                         "10k-500k triangles, 128^2-1024^2 px, 4-256 spp, depth 4-12, mis",
-            "jobs": len(table), "triangles_total": triangles,
+            "jobs": len(table),
+            "triangles_total": sum(sc.job_scene_triangles(j["triangles"]) for j in table),
             "samples_per_step": sum(j["width"] * j["height"] * j["samples_per_pixel"] for j in table),
             "job_table_seed": TABLE_SEED, "mode": "mis", "roulette_depth": 3,
-            "bvh": "GPU binned SAH with split references",
             "l2": "no flush: scenes (tens of millions of triangles) and per-wave path state "
                   "(GBs) exceed the 126 MB L2"}
 
@@ -313,8 +315,10 @@ def run_reference(args):
     line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * seconds / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": config(table, sum(j["triangles"] for j in table)), "impl": "reference",
+            "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config(table), "impl": "reference",
+            "engine": "CPU oracle (the reference algorithm restated in FP64 C++), the reference's "
+                      "serial SAH builder, tile-parallel render on the host threads",
             "cpu_baseline": {"value": value, "unit": METRIC, "cores": cpu_threads(),
                              "kind": "port",
                              "sample": sample.describe(samples // max(1, args.steps),
@@ -383,6 +387,157 @@ def serve(api, scenes, table, seconds, rng, rate=SERVE_RATE):
                             "after arrival"}
 
 
+def quintile_legs(api, jobs, tuned, plain):
+    """Batched vs plain per fifth of the mix by samples per job (smallest first): where batching
+    pays and where the plain path already fills the GPU."""
+    order = sorted(range(len(jobs)), key=lambda k: jobs[k].render.width * jobs[k].render.height *
+                   jobs[k].render.samples_per_pixel)
+    out = []
+    for q in range(5):
+        part = [jobs[k] for k in order[q * len(jobs) // 5:(q + 1) * len(jobs) // 5]]
+        if not part:
+            continue
+        counts = [j.render.width * j.render.height * j.render.samples_per_pixel for j in part]
+        _, codes, info = api.render_batch(part, tuned, copy_images=False)
+        assert all(c == 0 for c in codes), codes
+        plain_s = plain(part)
+        out.append({"jobs": len(part), "samples": sum(counts),
+                    "samples_per_job": [min(counts), max(counts)],
+                    "batched": sum(counts) / info["device_seconds"] / 1e6,
+                    "plain": sum(counts) / plain_s / 1e6,
+                    "batched_vs_plain": plain_s / info["device_seconds"], "unit": METRIC})
+    return out
+
+
+def preview_leg(api, jobs, tuned, plain):
+    """Preview-sized renders of the same scenes (128x128, 4 spp, each job's depth): the regime in
+    which one launch sequence per job leaves most of the GPU idle."""
+    tiny = [api.BatchJob(j.scene, api.RenderSettings(128, 128, 4, j.render.seed), j.integrator)
+            for j in jobs]
+    tiny_samples = sum(j.render.width * j.render.height * j.render.samples_per_pixel for j in tiny)
+    try:
+        api.render_batch(tiny, tuned, copy_images=False)  # warm-up
+        _, codes, info = api.render_batch(tiny, tuned, copy_images=False)
+        assert all(c == 0 for c in codes), codes
+        plain(tiny[:4])
+        tiny_plain = plain(tiny)
+        return {"jobs": len(tiny), "samples": tiny_samples, "render": "128x128, 4 spp",
+                "batched": tiny_samples / info["device_seconds"] / 1e6,
+                "plain": tiny_samples / tiny_plain / 1e6,
+                "batched_vs_plain": tiny_plain / info["device_seconds"], "unit": METRIC}
+    except Exception as error:  # a secondary leg: report it, keep the line
+        return {"error": f"{type(error).__name__}: {error}"}
+
+
+def timed_frames(tracer, render_settings, out, stream, count=1):
+    """Device milliseconds of `count` frames after one warm-up frame (CUDA events on `stream`)."""
+    import torch
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    tracer.render_device(render_settings[0], out.data_ptr(), stream.cuda_stream)
+    e0.record(stream)
+    for r in render_settings[:count]:
+        tracer.render_device(r, out.data_ptr(), stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1)
+
+
+LARGE_BAND = (532, 548)
+
+
+def large_frame_leg(api, sc, stream, with_cpu):
+    """Config 2: the 1.02M-triangle frame, 1920x1080, 64 spp, depth 12, GPU-built tree (reference
+    builder options); the CPU oracle renders a 16-row band of the same frame in the same run."""
+    import torch
+    snap = sc.large_scene().snapshot()
+    large = api.Scene(snap)
+    frame_render = api.RenderSettings(1920, 1080, 64, 1)
+    frame_tracer = api.PathTracer(large, api.IntegratorSettings("mis", 12, True, 3))
+    frame = torch.empty(1920 * 1080 * 3, dtype=torch.float32, device="cuda")
+    frame_ms = timed_frames(frame_tracer, [frame_render], frame, stream)
+    out = {"workload": "1920x1080 64 spp depth 12, 1.02M triangles (reference builder)",
+           "ms": frame_ms, "value": 1920 * 1080 * 64 / frame_ms / 1e3, "unit": METRIC,
+           "bvh_build_ms": 1e3 * large.build_seconds()}
+    large.close()
+    if with_cpu:
+        from oracle import pyoracle
+        o = pyoracle.OracleScene(snap, pyoracle.integrator("mis", 12, True, 3))
+        t0 = time.perf_counter()
+        o.render(frame_render.c(), threads=cpu_threads(), rows=LARGE_BAND, statistics=False)
+        seconds = time.perf_counter() - t0
+        band = (LARGE_BAND[1] - LARGE_BAND[0]) * 1920 * 64
+        out["cpu_band"] = {"value": band / seconds / 1e6, "unit": METRIC, "cores": cpu_threads(),
+                           "kind": "port", "rows": list(LARGE_BAND), "seconds": seconds,
+                           "full_frame_seconds_extrapolated": seconds * 1080 / (LARGE_BAND[1] -
+                                                                                LARGE_BAND[0]),
+                           "sample": "rows 532-548 of the frame at full spp (the oracle's "
+                                     "reference-builder tree; build not timed); the full "
+                                     "frame's time extrapolated by row count"}
+        out["gpu_vs_cpu"] = out["value"] / out["cpu_band"]["value"]
+    return out
+
+
+def large_frame_sharded(api, sc, rank, world):
+    """Config 2 split into one row band per rank (mr_render_rows) and gathered on rank 0:
+    the slowest rank's band time (host clock, after a barrier) plus the gather."""
+    import torch
+    import torch.distributed as dist
+    from minirender_b200 import shard
+    large = api.Scene(sc.large_scene().snapshot())
+    tracer = api.PathTracer(large, api.IntegratorSettings("mis", 12, True, 3))
+    render = api.RenderSettings(1920, 1080, 64, 1)
+    shard.render_frame_sharded(tracer, render)  # warm-up
+    dist.barrier()
+    t0 = time.perf_counter()
+    image = shard.render_frame_sharded(tracer, render)
+    seconds = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device="cuda")
+    dist.all_reduce(seconds, op=dist.ReduceOp.MAX)
+    large.close()
+    ms = 1e3 * float(seconds.item())
+    out = {"workload": "1920x1080 64 spp depth 12, 1.02M triangles, one row band per rank "
+                       "gathered on rank 0", "ms": ms, "value": 1920 * 1080 * 64 / ms / 1e3,
+           "unit": METRIC, "ranks": world}
+    if rank == 0:
+        out["image_mean"] = float(image.mean())
+    return out
+
+
+def config1_leg(api, sc, stream, with_cpu):
+    """Config 1: the 36-triangle Cornell box at 512x512, 16 spp, depth 8, MIS, roulette from depth
+    3, seeds 1-3, on the plain GPU path (device time), end to end through PathTracer.render (image
+    in host memory), and the full frame of seed 1 on the CPU oracle in the same run."""
+    import torch
+    scene = api.Scene(sc.cornell_box().snapshot())
+    settings = api.IntegratorSettings("mis", 8, True, 3)
+    tracer = api.PathTracer(scene, settings)
+    renders = [api.RenderSettings(512, 512, 16, seed) for seed in (1, 2, 3)]
+    out_buf = torch.empty(512 * 512 * 3, dtype=torch.float32, device="cuda")
+    samples = 512 * 512 * 16
+    ms = timed_frames(tracer, renders, out_buf, stream, count=3)
+    tracer.render(renders[0], statistics=False)
+    t0 = time.perf_counter()
+    for r in renders:
+        tracer.render(r, statistics=False)
+    e2e_seconds = time.perf_counter() - t0
+    out = {"workload": "Cornell box, 36 triangles, 512x512, 16 spp, depth 8, mis, seeds 1-3",
+           "ms_per_frame": ms / 3, "value": 3 * samples / ms / 1e3, "unit": METRIC,
+           "e2e": {"value": 3 * samples / e2e_seconds / 1e6, "unit": METRIC,
+                   "d2h_bytes_per_frame": 512 * 512 * 12,
+                   "call": "mr_render (PathTracer::render) into host memory, per frame"}}
+    scene.close()
+    if with_cpu:
+        from oracle import pyoracle
+        o = pyoracle.OracleScene(sc.cornell_box().snapshot(), pyoracle.integrator("mis", 8, True, 3))
+        t0 = time.perf_counter()
+        o.render(renders[0].c(), threads=cpu_threads(), statistics=False)
+        seconds = time.perf_counter() - t0
+        out["cpu"] = {"value": samples / seconds / 1e6, "unit": METRIC, "cores": cpu_threads(),
+                      "kind": "port", "seconds": seconds,
+                      "sample": "the full 512x512x16 frame of seed 1"}
+        out["e2e_vs_cpu"] = out["e2e"]["value"] / out["cpu"]["value"]
+    return out
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -402,20 +557,30 @@ def run_ours(args):
             dist.barrier()
 
     table = job_table(args.jobs)
-    for job in table:  # weak scaling: every rank its own render seeds
-        job["render_seed"] += 1000 * rank
+    # One job table for the whole job. With N ranks it is partitioned by shard.partition_jobs
+    # (longest processing time first on samples x depth) and every rank renders only its share:
+    # strong scaling, no collective on the data path.
+    mine = list(range(len(table)))
+    if world > 1:
+        from minirender_b200 import shard
+        costs = [j["width"] * j["height"] * j["samples_per_pixel"] * (j["maximum_depth"] + 1)
+                 for j in table]
+        mine = shard.partition_jobs(costs, world)[rank]
+    samples_total = sum(j["width"] * j["height"] * j["samples_per_pixel"] for j in table)
     t0 = time.perf_counter()
-    snaps = [job_document(j).snapshot() for j in table]
+    snaps = [job_document(table[k]).snapshot() for k in mine]
     gen_seconds = time.perf_counter() - t0
     t0 = time.perf_counter()
     scenes = [api.Scene(s, split_references=True) for s in snaps]
     torch.cuda.synchronize()
     scene_seconds = time.perf_counter() - t0
-    triangles = sum(s.triangle_count for s in snaps)
-    jobs = [api.BatchJob(s, api.RenderSettings(j["width"], j["height"], j["samples_per_pixel"],
-                                               j["render_seed"]),
-                         api.IntegratorSettings("mis", j["maximum_depth"], True, 3))
-            for s, j in zip(scenes, table)]
+    if world == 1:
+        assert sum(s.triangle_count for s in snaps) == config(table)["triangles_total"]
+    jobs = [api.BatchJob(s, api.RenderSettings(table[k]["width"], table[k]["height"],
+                                               table[k]["samples_per_pixel"],
+                                               table[k]["render_seed"]),
+                         api.IntegratorSettings("mis", table[k]["maximum_depth"], True, 3))
+            for s, k in zip(scenes, mine)]
     samples = sum(j.render.width * j.render.height * j.render.samples_per_pixel for j in jobs)
 
     # Autotuner on a calibration subset (every fourth job at 1/16 of its samples), untimed.
@@ -424,13 +589,17 @@ def run_ours(args):
                                                       j.render.seed), j.integrator)
              for j in jobs[::4]]
     t0 = time.perf_counter()
-    if args.no_autotune:
+    if args.no_autotune or not calib:
         tuned, tuned_rate = api.BatchSettings(), 0.0
     else:
         tuned, tuned_rate = api.autotune(calib)
     tune_seconds = time.perf_counter() - t0
 
     def step():
+        if not jobs:  # a rank without a share (more ranks than jobs)
+            return {"device_seconds": 0.0, "kernel_launches": 0, "waves": 0,
+                    "paths": {"paths": 0, "scattering_events": 0, "roulette_terminations": 0,
+                              "shadow_rays": 0}}
         _, codes, info = api.render_batch(jobs, tuned, copy_images=False)
         assert all(c == 0 for c in codes), codes
         return info
@@ -461,94 +630,49 @@ def run_ours(args):
     if world > 1:
         dist.all_reduce(worst, op=dist.ReduceOp.MAX)
     worst = float(worst.item())
-    value = world * samples * args.steps / worst / 1e6
+    value = samples_total * args.steps / worst / 1e6
+    own_batched_seconds = device_seconds / args.steps  # this rank's share, one step
+    if world > 1:  # counters of the whole job
+        totals = torch.tensor([launches, waves, *rays.values()], dtype=torch.float64,
+                              device="cuda")
+        dist.all_reduce(totals)
+        launches, waves = int(totals[0].item()), int(totals[1].item())
+        rays = {k: int(totals[2 + i].item()) for i, k in enumerate(rays)}
 
     # Plain path on the same jobs: one mr_render_device call per job.
     stream = torch.cuda.current_stream()
-    image = torch.empty(max(j.render.width * j.render.height for j in jobs) * 3,
-                        dtype=torch.float32, device="cuda")
-    for j in jobs[:4]:
-        api.PathTracer(j.scene, j.integrator).render_device(j.render, image.data_ptr(),
-                                                            stream.cuda_stream)
-    torch.cuda.synchronize()
-    assert lib.mr_set_kernel_timing(1) == 0
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for j in jobs:
-        api.PathTracer(j.scene, j.integrator).render_device(j.render, image.data_ptr(),
-                                                            stream.cuda_stream)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    plain_seconds = e0.elapsed_time(e1) / 1e3
+    image = torch.empty(max([j.render.width * j.render.height for j in jobs] or [1]) * 3,
+                        dtype=torch.float32, device="cuda")
+
+    def plain(part):
+        """Device seconds of one mr_render_device call per job, on the caller's stream."""
+        e0.record(stream)
+        for j in part:
+            api.PathTracer(j.scene, j.integrator).render_device(j.render, image.data_ptr(),
+                                                                stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 1e3
+
+    plain(jobs[:4])
+    assert lib.mr_set_kernel_timing(1) == 0
+    plain_seconds = plain(jobs)
     k_launches, ksec, all_launches = C.c_uint64(), C.c_double(), C.c_uint64()
     counted = _abi.TraceStatistics()
     lib.mr_kernel_timing(C.byref(k_launches), C.byref(ksec), C.byref(counted),
                          C.byref(all_launches))
     lib.mr_set_kernel_timing(0)
-    plain_value = samples / plain_seconds / 1e6
+    plain_value = samples / max(plain_seconds, 1e-9) / 1e6
 
-    # The smaller half of the mix (by samples), batched and plain: the jobs batching is for.
-    order = sorted(range(len(jobs)), key=lambda k: jobs[k].render.width * jobs[k].render.height *
-                   jobs[k].render.samples_per_pixel)
-    small = [jobs[k] for k in order[: len(jobs) // 2]]
-    small_samples = sum(j.render.width * j.render.height * j.render.samples_per_pixel for j in small)
-    api.render_batch(small, tuned, copy_images=False)  # warm-up
-    _, _, info = api.render_batch(small, tuned, copy_images=False)
-    small_batched = info["device_seconds"]
-    e0.record(stream)
-    for j in small:
-        api.PathTracer(j.scene, j.integrator).render_device(j.render, image.data_ptr(),
-                                                            stream.cuda_stream)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    small_plain = e0.elapsed_time(e1) / 1e3
-    small_jobs = {"jobs": len(small), "samples": small_samples,
-                  "batched": small_samples / small_batched / 1e6,
-                  "plain": small_samples / small_plain / 1e6,
-                  "batched_vs_plain": small_plain / small_batched, "unit": METRIC}
-
-    # Preview-sized renders of the same scenes (128x128, 4 spp, each job's depth): the regime in
-    # which one launch sequence per job leaves most of the GPU idle.
-    tiny = [api.BatchJob(j.scene, api.RenderSettings(128, 128, 4, j.render.seed), j.integrator)
-            for j in jobs]
-    tiny_samples = sum(j.render.width * j.render.height * j.render.samples_per_pixel for j in tiny)
-    try:
-        api.render_batch(tiny, tuned, copy_images=False)  # warm-up
-        _, codes, info = api.render_batch(tiny, tuned, copy_images=False)
-        assert all(c == 0 for c in codes), codes
-        tiny_batched = info["device_seconds"]
-        for j in tiny[:4]:
-            api.PathTracer(j.scene, j.integrator).render_device(j.render, image.data_ptr(),
-                                                                stream.cuda_stream)
-        e0.record(stream)
-        for j in tiny:
-            api.PathTracer(j.scene, j.integrator).render_device(j.render, image.data_ptr(),
-                                                                stream.cuda_stream)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        tiny_plain = e0.elapsed_time(e1) / 1e3
-        tiny_jobs = {"jobs": len(tiny), "samples": tiny_samples, "render": "128x128, 4 spp",
-                     "batched": tiny_samples / tiny_batched / 1e6,
-                     "plain": tiny_samples / tiny_plain / 1e6,
-                     "batched_vs_plain": tiny_plain / tiny_batched, "unit": METRIC}
-    except Exception as error:  # a secondary leg: report it, keep the line
-        tiny_jobs = {"error": f"{type(error).__name__}: {error}"}
-
-    # The single 1M-triangle frame (plain path), after one warm-up frame.
-    large = api.Scene(sc.large_scene().snapshot())
-    frame_render = api.RenderSettings(1920, 1080, 64, 1 + rank)
-    frame_tracer = api.PathTracer(large, api.IntegratorSettings("mis", 12, True, 3))
-    frame = torch.empty(1920 * 1080 * 3, dtype=torch.float32, device="cuda")
-    frame_tracer.render_device(frame_render, frame.data_ptr(), stream.cuda_stream)
-    e0.record(stream)
-    frame_tracer.render_device(frame_render, frame.data_ptr(), stream.cuda_stream)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    frame_ms = e0.elapsed_time(e1)
-    large_frame = {"workload": "1920x1080 64 spp depth 12, 1.02M triangles (reference builder)",
-                   "ms": frame_ms, "value": 1920 * 1080 * 64 / frame_ms / 1e3, "unit": METRIC,
-                   "bvh_build_ms": 1e3 * large.build_seconds()}
-    large.close()
+    quintiles = tiny_jobs = large_frame = config1 = None
+    if world == 1:
+        quintiles = quintile_legs(api, jobs, tuned, plain)
+        tiny_jobs = preview_leg(api, jobs, tuned, plain)
+        large_frame = large_frame_leg(api, sc, stream, not args.no_cpu_baseline)
+        config1 = config1_leg(api, sc, stream, not args.no_cpu_baseline)
+    else:
+        large_frame = large_frame_sharded(api, sc, rank, world)
 
     # End to end through the public API from pinned host memory.
     e2e_value, h2d, d2h, e2e_phase = None, 0, 0, None
@@ -563,13 +687,22 @@ def run_ours(args):
 
         def e2e_step():
             # Scenes are built on 8 host threads: construction runs on its own stream with
-            # stream-ordered buffers, so builds overlap one another on the GPU.
+            # stream-ordered buffers, so builds overlap one another on the GPU. With N ranks each
+            # renders its share and rank 0 gathers every image (the one collective).
             t0 = time.perf_counter()
             fresh = list(builders.map(lambda s: api.Scene(s, split_references=True), snaps))
             t1 = time.perf_counter()
             batch = [api.BatchJob(f, j.render, j.integrator) for f, j in zip(fresh, jobs)]
-            _, codes, _ = api.render_batch(batch, tuned)
-            assert all(c == 0 for c in codes), codes
+            if batch:
+                images, codes, _ = api.render_batch(batch, tuned)
+                assert all(c == 0 for c in codes), codes
+            else:
+                images = []
+            if world > 1:
+                gathered = [None] * world if rank == 0 else None
+                dist.gather_object(list(zip(mine, images)), gathered, dst=0)
+                if rank == 0:
+                    assert sum(len(g) for g in gathered) == len(table)
             phase["build"] += t1 - t0
             phase["render"] += time.perf_counter() - t1
             for f in fresh:
@@ -587,8 +720,12 @@ def run_ours(args):
         barrier()
         if world > 1:
             dist.all_reduce(e2e_seconds, op=dist.ReduceOp.MAX)
-        e2e_value = world * samples * args.steps / float(e2e_seconds.item()) / 1e6
+        e2e_value = samples_total * args.steps / float(e2e_seconds.item()) / 1e6
         e2e_phase = phase
+        if world > 1:  # every rank's bytes: the job's totals
+            counts = torch.tensor([h2d, d2h], dtype=torch.float64, device="cuda")
+            dist.all_reduce(counts)
+            h2d, d2h = int(counts[0].item()), int(counts[1].item())
 
     serving = sustainable = None
     if world == 1 and not args.no_serve:
@@ -630,15 +767,24 @@ def run_ours(args):
     max_mhz = (clock_info or {}).get("sm_max_mhz") or SM_MAX_MHZ
     fp32_peak = props.multi_processor_count * 128 * 2 * max_mhz * 1e6 / 1e12
     flops_achieved = flops / ksec.value / 1e12 if ksec.value > 0 else 0.0
-    traffic = None
+    traffic, profile = None, {}
     tfile = os.path.join(ROOT, "profiles", "trace_kernel_traffic.txt")
     if os.path.exists(tfile):
         with open(tfile) as f:
-            ratio = json.load(f).get("dram_bytes_per_algorithmic_byte")
+            profile = json.load(f)
+        ratio = profile.get("dram_bytes_per_algorithmic_byte")
         # DRAM bytes per algorithmic byte of the captured launches, applied to this run's
         # average launch.
         if ratio:
             traffic = ratio * per_launch
+    avg_launch_s = ksec.value / max(1, k_launches.value)
+    dram_gbs = traffic / avg_launch_s / 1e9 if traffic and avg_launch_s > 0 else None
+    # What bounds the kernel: the algorithmic bytes are mostly served by L1/L2, so the DRAM side
+    # runs far below the copy peak; the profile's issue and lane figures say why.
+    limiter = ("issue and latency (divergent lanes), not DRAM: "
+               f"{profile.get('lanes_active_per_instruction', '?')} of 32 lanes active per "
+               f"instruction, issue active {profile.get('issue_active', '?')} of cycles "
+               f"({profile.get('profile', 'profiles/trace_kernel_traffic.txt')})")
 
     line = None
     if rank == 0:
@@ -646,9 +792,10 @@ def run_ours(args):
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
             "steps": args.steps, "warmup": max(3, args.warmup),
             "ms_per_step": 1e3 * worst / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {**config(table, triangles),
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {**config(table),
                        "engine": "batched: mr_render_batch, jobs packed into shared waves",
+                       "bvh": "GPU binned SAH with split references",
                        "autotuned": {"wave_paths": tuned.wave_paths,
                                      "concurrent_waves": tuned.concurrent_waves,
                                      "sort_threshold": tuned.sort_threshold,
@@ -658,7 +805,7 @@ def run_ours(args):
                        "wall_ms_per_step": 1e3 * wall / args.steps,
                        "waves_per_step": waves / args.steps,
                        "rays": {"per_step": {kind: n // args.steps for kind, n in rays.items()},
-                                "Grays_per_s": world * sum(rays.values()) / worst / 1e9,
+                                "Grays_per_s": sum(rays.values()) / worst / 1e9,
                                 "counted": "primary = camera paths, extension = scattering "
                                            "events that survived roulette, shadow = shadow "
                                            "rays (engine path statistics)"},
@@ -666,9 +813,10 @@ def run_ours(args):
                        "plain_gpu": {"value": plain_value, "unit": METRIC,
                                      "ms_per_step": 1e3 * plain_seconds,
                                      "engine": "mr_render_device, one job per call"},
-                       "batched_vs_plain": value / plain_value,
-                       "small_jobs": small_jobs,
+                       "batched_vs_plain": plain_seconds / max(own_batched_seconds, 1e-9),
+                       "quintiles": quintiles,
                        "preview_jobs": tiny_jobs,
+                       "config1": config1,
                        "serving": serving, "serving_sustainable": sustainable,
                        "large_frame": large_frame, "stress": stress},
             "roofline": {"bound": "hbm", "kernel": "trace_kernel (nearest-hit + shadow "
@@ -679,6 +827,10 @@ def run_ours(args):
                          "launches": k_launches.value,
                          "avg_launch_ms": 1e3 * ksec.value / max(1, k_launches.value),
                          "bytes_model": "24 B per bounds test + 36 B per triangle test",
+                         "dram": {"achieved": dram_gbs, "unit": "GB/s",
+                                  "frac": dram_gbs / peak if dram_gbs else None,
+                                  "from": "traffic per launch / average launch time"},
+                         "limiter": limiter,
                          "fp32": {"achieved": flops_achieved, "peak": fp32_peak,
                                   "unit": "TFLOP/s", "frac": flops_achieved / fp32_peak,
                                   "peak_source": "nominal: SMs x 128 FP32 lanes x 2 x max SM clock",

@@ -503,15 +503,28 @@ def stress_scene(seed: int = 5, count: int = 4000, variants: int = 64) -> SceneD
     return doc
 
 
+_PER_SPHERE = {0: 20, 1: 80, 2: 320, 3: 1280, 4: 5120}
+
+
+def _job_spheres(triangles: int) -> tuple[int, int]:
+    """Subdivision level and sphere count of a job scene of about `triangles` triangles."""
+    budget = max(0, triangles - 36)
+    level = 3 if budget < 200_000 else 4
+    return level, max(1, budget // _PER_SPHERE[level])
+
+
+def job_scene_triangles(triangles: int) -> int:
+    """The exact triangle count job_scene(triangles, seed) builds (any seed)."""
+    level, n = _job_spheres(triangles)
+    return 36 + n * _PER_SPHERE[level]
+
+
 def job_scene(triangles: int, seed: int) -> SceneDocument:
     """A Cornell shell filled with displaced icospheres up to about `triangles` triangles
     (the uneven job table's scenes)."""
     rng = np.random.default_rng(seed)
     doc = cornell_box()
-    per_sphere = {0: 20, 1: 80, 2: 320, 3: 1280, 4: 5120}
-    budget = max(0, triangles - 36)
-    level = 3 if budget < 200_000 else 4
-    n = max(1, budget // per_sphere[level])
+    level, n = _job_spheres(triangles)
     variants = min(n, 8)
     first = len(doc.meshes)
     for k in range(variants):
