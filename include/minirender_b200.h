@@ -157,7 +157,7 @@ typedef struct mr_scene_desc {
 /* SceneBvh::Node (include/minirender/render/bvh.hpp:81-86), the reference's flat node layout.
  * Leaf: count > 0 and [first, first+count) indexes `order`. Interior: count == 0, `first` is
  * the left child and `right` the right child. Primitive ids enumerate instances in order and
- * their triangles in order, as in SceneBvh's constructor (src/render/bvh.cpp:163-199). */
+ * their triangles in order, as in SceneBvh's constructor (src/render/bvh.cpp:53-89). */
 typedef struct mr_bvh_node {
     float    minimum[3];
     float    maximum[3];
@@ -284,10 +284,10 @@ size_t mr_last_error(char* buffer, size_t capacity);
 /* ---- scene ------------------------------------------------------------------------------ */
 
 /* Validates the snapshot, uploads it to the current CUDA device and builds everything the
- * reference's PathTracer constructor builds (src/render/path_tracer.cpp:244-253): the SceneBvh
- * (src/render/bvh.cpp:141-209; here the GPU binned-SAH builder, or `bvh` when non-null, which
+ * reference's PathTracer constructor builds (src/render/path_tracer.cpp:111-120): the SceneBvh
+ * (src/render/bvh.cpp:31-99; here the GPU binned-SAH builder, or `bvh` when non-null, which
  * must be the reference layout of the same primitives), the LightSampler
- * (src/render/light.cpp:340-407) and the MediumField (src/render/medium.cpp:228-231). */
+ * (src/render/light.cpp:197-264) and the MediumField (src/render/medium.cpp:145-148). */
 mr_status mr_scene_create(const mr_scene_desc* desc, const mr_bvh_desc* bvh, mr_scene** scene);
 
 /* Builder options. No reference counterpart: the reference bins whole triangles only. */
@@ -314,7 +314,7 @@ mr_status mr_scene_destroy(mr_scene* scene);
 mr_status mr_scene_bvh_statistics(const mr_scene* scene, mr_bvh_statistics* statistics);
 
 /* Surface-area-heuristic cost of the scene's BVH with the reference builder's constants
- * (C_T = C_I = 1, src/render/bvh.cpp:244-245): sum over interior nodes of A(node)/A(root) plus
+ * (C_T = C_I = 1, src/render/bvh.cpp:134-135): sum over interior nodes of A(node)/A(root) plus
  * sum over leaves of count * A(leaf)/A(root). No single reference function computes the
  * whole-tree figure; it is the cost the reference's split search minimises. */
 mr_status mr_scene_sah_cost(const mr_scene* scene, double* cost);
@@ -333,23 +333,23 @@ mr_status mr_scene_build_seconds(const mr_scene* scene, double* seconds);
 
 /* ---- queries ---------------------------------------------------------------------------- */
 
-/* SceneBvh::intersect (src/render/bvh.cpp:482-488) for `count` rays: nearest hit in the closed
+/* SceneBvh::intersect (src/render/bvh.cpp:372-378) for `count` rays: nearest hit in the closed
  * interval, ties to the lowest primitive id, single-sided culling. */
 mr_status mr_intersect(const mr_scene* scene, const mr_ray* rays, size_t count, mr_hit* hits,
                        mr_trace_statistics* statistics);
 
-/* SceneBvh::occluded (src/render/bvh.cpp:490-494) for `count` rays; occluded[i] is 0 or 1. */
+/* SceneBvh::occluded (src/render/bvh.cpp:380-384) for `count` rays; occluded[i] is 0 or 1. */
 mr_status mr_occluded(const mr_scene* scene, const mr_ray* rays, size_t count, uint8_t* occluded,
                       mr_trace_statistics* statistics);
 
-/* PathTracer::trace (src/render/path_tracer.cpp:286-499) for `count` independent paths. The
+/* PathTracer::trace (src/render/path_tracer.cpp:153-366) for `count` independent paths. The
  * sampler of path i is Sampler::for_sample(keys[3i], keys[3i+1], keys[3i+2])
- * (src/core/sampling.cpp:124-127); rays[i] carries the primary interval. */
+ * (src/core/sampling.cpp:43-46); rays[i] carries the primary interval. */
 mr_status mr_trace_paths(const mr_scene* scene, const mr_integrator_settings* integrator,
                          const mr_ray* rays, const uint64_t* keys, size_t count,
                          float* radiance, mr_path_statistics* statistics);
 
-/* PathTracer::sample_pixel (src/render/path_tracer.cpp:501-519) for `count` (x, y, sample)
+/* PathTracer::sample_pixel (src/render/path_tracer.cpp:368-386) for `count` (x, y, sample)
  * triples (`pixels` holds x, y pairs). Writes the radiance and, when `rays` is non-null, the
  * primary camera ray with its clip interval. */
 mr_status mr_sample_pixels(const mr_scene* scene, const mr_integrator_settings* integrator,
@@ -361,7 +361,7 @@ mr_status mr_sample_pixels(const mr_scene* scene, const mr_integrator_settings* 
  * and reports, per sample, the first shadow ray its path traced (origin, direction, interval
  * [0, limit]) in `shadow_rays`, has_shadow[i] = 1 when it traced one, and occluded[i] = the
  * any-hit result. No reference counterpart (the reference traces the same ray inside
- * PathTracer::shadow_transmittance, src/render/path_tracer.cpp:259-284). */
+ * PathTracer::shadow_transmittance, src/render/path_tracer.cpp:126-151). */
 mr_status mr_capture_shadow_rays(const mr_scene* scene, const mr_integrator_settings* integrator,
                                  const mr_render_settings* render, const uint32_t* pixels,
                                  const uint64_t* samples, size_t count, mr_ray* shadow_rays,
@@ -391,7 +391,7 @@ mr_status mr_trace_paths_static(const mr_scene* scene, const mr_integrator_setti
 
 /* ---- render ----------------------------------------------------------------------------- */
 
-/* PathTracer::render (src/render/path_tracer.cpp:521-538): writes width*height*3 floats of
+/* PathTracer::render (src/render/path_tracer.cpp:388-405): writes width*height*3 floats of
  * linear RGB, row-major, origin top-left (include/minirender/core/image.hpp). Host buffer. */
 mr_status mr_render(const mr_scene* scene, const mr_integrator_settings* integrator,
                     const mr_render_settings* render, float* rgb, mr_path_statistics* statistics);
@@ -413,7 +413,7 @@ mr_status mr_render_rows(const mr_scene* scene, const mr_integrator_settings* in
                          const mr_render_settings* render, uint64_t row_begin, uint64_t row_end,
                          float* rgb, mr_path_statistics* statistics);
 
-/* display_image (src/render/path_tracer.cpp:540-557): exposure + Reinhard on a host image. */
+/* display_image (src/render/path_tracer.cpp:407-424): exposure + Reinhard on a host image. */
 mr_status mr_display_image(const float* linear, uint64_t width, uint64_t height, double exposure,
                            float* display);
 

@@ -84,7 +84,7 @@ class PathTracer {
             throw std::invalid_argument("PathTracer requires a scene");
         }
     }
-    // PathTracer::render (src/render/path_tracer.cpp:521-538).
+    // PathTracer::render (src/render/path_tracer.cpp:388-405).
     Image render(const mr_render_settings& settings, mr_path_statistics* statistics = nullptr) const {
         Image image{static_cast<std::size_t>(settings.width), static_cast<std::size_t>(settings.height), {}};
         image.rgb.resize(3 * image.width * image.height);

@@ -85,7 +85,7 @@ def pack_rays(origins, directions, minimum, maximum) -> np.ndarray:
 
 class Scene:
     """A snapshot uploaded to the current CUDA device with its BVH, lights and media
-    (the construction half of PathTracer, src/render/path_tracer.cpp:244-253)."""
+    (the construction half of PathTracer, src/render/path_tracer.cpp:111-120)."""
 
     def __init__(self, snapshot: Snapshot | SceneDocument, bvh: _abi.BvhDesc | None = None,
                  split_references: bool = False, split_factor: float = 0.0,
@@ -139,7 +139,7 @@ class Scene:
               self.lib)
         return nodes, order[:prims_n.value], nodes_n.value
 
-    # ---- SceneBvh queries (src/render/bvh.cpp:482-494) ----
+    # ---- SceneBvh queries (src/render/bvh.cpp:372-384) ----
 
     def intersect(self, origins, directions, minimum=1e-5, maximum=np.inf):
         rays = pack_rays(origins, directions, minimum, maximum)
@@ -258,7 +258,7 @@ class PathTracer:
 
 
 def display_image(linear: np.ndarray, exposure: float = 0.0) -> np.ndarray:
-    """display_image (src/render/path_tracer.cpp:540-557)."""
+    """display_image (src/render/path_tracer.cpp:407-424)."""
     lib = load_library()
     linear = _f32(linear)
     h, w = linear.shape[:2]

@@ -76,7 +76,7 @@ template <typename F> mr_status guarded(F&& f) {
     }
 }
 
-// RayQuery constructor and RayInterval::validate (src/render/intersection.cpp:22-26,123-130).
+// RayQuery constructor and RayInterval::validate (src/render/intersection.cpp:22-26,52-61).
 void validate_ray(const mr_ray& r) {
     for (int a = 0; a < 3; ++a) {
         require(std::isfinite(r.origin[a]) && std::isfinite(r.direction[a]),
@@ -523,7 +523,7 @@ mr_status mr_scene_sah_cost(const mr_scene* scene, double* cost) {
         }
         std::vector<mr_bvh_node> nodes(n);
         MR_CUDA(cudaMemcpy(nodes.data(), s.ref_nodes.ptr, n * sizeof(mr_bvh_node), cudaMemcpyDeviceToHost));
-        // Areas as the reference computes them (Bounds3::surface_area, intersection.cpp:115-121).
+        // Areas as the reference computes them (Bounds3::surface_area, intersection.cpp:44-50).
         const auto area = [](const mr_bvh_node& b) {
             const double ex = double(b.maximum[0]) - b.minimum[0];
             const double ey = double(b.maximum[1]) - b.minimum[1];

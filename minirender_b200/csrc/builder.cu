@@ -1,6 +1,6 @@
 // builder.cu — GPU binned-SAH BVH builder.
 //
-// The algorithm is the reference's recursive builder (src/render/bvh.cpp:211-306) evaluated
+// The algorithm is the reference's recursive builder (src/render/bvh.cpp:101-196) evaluated
 // breadth-first on the GPU: 12 centroid bins per axis, C_T = C_I = 1, a leaf when a node holds at
 // most 4 primitives, sits at depth 48, has no split with nonempty sides, or no split cheaper than
 // the leaf cost (its primitive count). Ties keep the first axis and split in the reference's
@@ -15,7 +15,7 @@
 //  - smaller nodes are finished by one warp each, depth-first in shared memory, with node
 //    indices taken from a range reserved per subtree (unused indices are squeezed out at the end).
 // All arithmetic is FP32. Surface areas are evaluated on extents scaled by a power of two so the
-// products cannot overflow (the reference uses double for the same reason, bvh.cpp:115-121).
+// products cannot overflow (the reference uses double for the same reason, intersection.cpp:44-50).
 #include <algorithm>
 #include <vector>
 
@@ -44,7 +44,7 @@ __device__ __forceinline__ float o2f(uint32_t o) {
 constexpr uint32_t kOrderedPosInf = 0xff800000u;  // f2o(+inf)
 constexpr uint32_t kOrderedNegInf = 0x007fffffu;  // f2o(-inf)
 
-// bin_index (src/render/bvh.cpp:133-137) in FP32.
+// bin_index (src/render/bvh.cpp:23-27) in FP32.
 __device__ __forceinline__ int bin_of(float c, float lo, float hi) {
     const float coordinate = (c - lo) / (hi - lo);
     const float scaled     = coordinate * static_cast<float>(kBins);
@@ -216,7 +216,7 @@ __global__ void bin_kernel(const Chunk* chunks, const uint32_t* order, const flo
     }
 }
 
-// SAH sweep over the 12 bins of the three axes (src/render/bvh.cpp:241-293).
+// SAH sweep over the 12 bins of the three axes (src/render/bvh.cpp:131-183).
 __device__ Split choose_split(const float* lo, const float* hi, const float* clo, const float* chi,
                               uint32_t count, const uint32_t (*bin_count)[kBins],
                               const float (*bin_lo)[kBins][3], const float (*bin_hi)[kBins][3]) {
@@ -466,7 +466,7 @@ __global__ void small_reserve_kernel(const Task* small, uint32_t count, uint32_t
 }
 
 // Small subtrees: one warp per task, depth-first in shared memory. Node indices are assigned in
-// pre-order from the task's reserved range (the reference's emplacement order, bvh.cpp:214-215).
+// pre-order from the task's reserved range (the reference's emplacement order, bvh.cpp:104-105).
 __global__ void __launch_bounds__(32 * kSmallWarps)
 small_build_kernel(const Task* small, uint32_t count, const uint32_t* ranges, uint32_t range_base,
                    uint32_t* order, const float4* plo, const float4* phi, const float4* pc,

@@ -14,7 +14,7 @@
 //              [1] = v1.xyz, flags (uint bits: kTriSingleSided | kTriMirrored | kind << 8)
 //              [2] = v2.xyz, 0
 //  - shading (per primitive, primitive order): 3 float4 = world-space unit corner normals
-//            (normalize(normal_to_world * n), src/render/bvh.cpp:429-430) with
+//            (normalize(normal_to_world * n), src/render/bvh.cpp:319-320) with
 //            w = instance index, triangle index, material index (uint bits).
 //  - materials, lights and the camera basis are small tables.
 #pragma once
@@ -33,7 +33,7 @@ enum TriFlags : unsigned {
 struct DeviceMaterial {
     f3       base_color;
     f3       emission;
-    float    alpha;  // roughness^2 (src/render/bsdf.cpp:216)
+    float    alpha;  // roughness^2 (src/render/bsdf.cpp:125)
     float    ior;
     uint32_t kind;
     uint32_t double_sided;

@@ -1,6 +1,6 @@
 // rng.cuh — the reference's per-(seed, pixel, sample) PCG32 streams on the GPU.
 //
-// Integer-exact restatement of src/core/sampling.cpp:108-146: SplitMix64 seeding, PCG32
+// Integer-exact restatement of src/core/sampling.cpp:28-65: SplitMix64 seeding, PCG32
 // XSH-RR output, two 32-bit outputs per 1-D sample. The reference forms a 53-bit double from
 // (u32 >> 5, u32 >> 6); here the same 53-bit integer is rounded once to FP32 (round to nearest)
 // and clamped below 1, so every sample is the FP32 rounding of the reference's double and the
@@ -45,7 +45,7 @@ struct Pcg32 {
         return p;
     }
 
-    // Sampler::for_sample (src/core/sampling.cpp:124-127).
+    // Sampler::for_sample (src/core/sampling.cpp:43-46).
     MR_HD static Pcg32 for_sample(uint64_t seed, uint64_t pixel, uint64_t sample) {
         return seeded(splitmix_finalize(seed ^ splitmix_finalize(pixel + 0x9e3779b97f4a7c15ULL)),
                       splitmix_finalize(sample + 0xd1b54a32d192ed03ULL) ^ splitmix_finalize(pixel));

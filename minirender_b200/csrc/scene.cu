@@ -1,9 +1,9 @@
 // scene.cu — validation, upload and device layout of a scene snapshot.
 //
-// Follows the reference's PathTracer construction (src/render/path_tracer.cpp:244-253):
-// snapshot validation (src/scene/scene.cpp:38-66,141-155,241-267; src/scene/medium.cpp:377-420),
-// world-space triangle flattening (src/render/bvh.cpp:141-209), BVH, light table
-// (src/render/light.cpp:340-407) and media. All arithmetic is FP32; the flattening uses
+// Follows the reference's PathTracer construction (src/render/path_tracer.cpp:111-120):
+// snapshot validation (src/scene/scene.cpp:38-66,141-155,241-267; src/scene/medium.cpp:31-65),
+// world-space triangle flattening (src/render/bvh.cpp:31-99), BVH, light table
+// (src/render/light.cpp:197-264) and media. All arithmetic is FP32; the flattening uses
 // explicit unfused multiply/add so host and device produce identical world vertices.
 #include <algorithm>
 #include <cmath>
@@ -20,7 +20,7 @@ namespace mr {
 namespace {
 
 // glm::vec3(object_to_world * glm::vec4(p, 1)) in float with GLM's evaluation order
-// (m0*x + m1*y) + (m2*z + m3*w) and no fused operations (src/render/bvh.cpp:178-179).
+// (m0*x + m1*y) + (m2*z + m3*w) and no fused operations (src/render/bvh.cpp:68-69).
 MR_HD f3 transform_point(const float* m, float x, float y, float z) {
 #ifdef __CUDA_ARCH__
     const auto row = [&](int r) {
@@ -301,7 +301,7 @@ void validate_mesh(const mr_mesh& m) {
     }
 }
 
-// MediumRegion / validate_medium_regions (src/scene/medium.cpp:377-420).
+// MediumRegion / validate_medium_regions (src/scene/medium.cpp:31-65).
 void validate_media(const mr_medium_region* media, uint32_t count) {
     require(count <= kMaxMedia, "Scene supports at most 32 medium regions");
     for (uint32_t i = 0; i < count; ++i) {
@@ -670,7 +670,7 @@ std::unique_ptr<Scene> create_scene(const mr_scene_desc& desc, const mr_bvh_desc
     MR_CUDA(cudaMemcpyAsync(scene->materials.ptr, materials.data(), materials.size() * sizeof(DeviceMaterial),
                             cudaMemcpyHostToDevice, stream));
 
-    // ---- lights (LightSampler constructor, src/render/light.cpp:340-407) ----
+    // ---- lights (LightSampler constructor, src/render/light.cpp:197-264) ----
     std::vector<DeviceLight> lights;
     std::vector<float>       weights;
     std::vector<uint32_t>    emitter_of_prim(std::max<uint32_t>(1, prims), kNone);
@@ -738,7 +738,7 @@ std::unique_ptr<Scene> create_scene(const mr_scene_desc& desc, const mr_bvh_desc
         lights.push_back(l);
         weights.push_back(projected_area * integral);
     }
-    // DiscreteDistribution (src/core/sampling.cpp:190-208) in FP32.
+    // DiscreteDistribution (src/core/sampling.cpp:109-127) in FP32.
     std::vector<float> cdf(weights.size() + 1, 0.0f);
     float maximum = 0;
     for (float w : weights) {

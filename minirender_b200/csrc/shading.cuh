@@ -9,7 +9,7 @@
 
 namespace mr {
 
-// ---- warps (src/core/sampling.cpp:148-188) ----
+// ---- warps (src/core/sampling.cpp:67-107) ----
 
 __device__ __forceinline__ void sample_disk(float ux, float uy, float& dx, float& dy) {
     const float sx = 2.0f * ux - 1.0f;
@@ -46,7 +46,7 @@ __device__ __forceinline__ f3 sample_triangle(float ux, float uy) {
     return {1.0f - root, root * (1.0f - uy), root * uy};
 }
 
-// ---- camera (src/scene/scene.cpp:171-199, src/render/path_tracer.cpp:501-519) ----
+// ---- camera (src/scene/scene.cpp:171-199, src/render/path_tracer.cpp:368-386) ----
 
 struct CameraRay {
     f3    origin, direction;
@@ -76,7 +76,7 @@ __device__ __forceinline__ CameraRay camera_ray(const CameraBasis& c, float u, f
     return r;
 }
 
-// ---- surface hit (src/render/bvh.cpp:412-480) ----
+// ---- surface hit (src/render/bvh.cpp:302-370) ----
 
 struct SurfaceHit {
     f3       position;
@@ -123,7 +123,7 @@ __device__ __forceinline__ SurfaceHit surface_hit(const DeviceScene& s, f3 direc
     return h;
 }
 
-// offset_origin (src/render/path_tracer.cpp:220-238) with FP32 error bounds.
+// offset_origin (src/render/path_tracer.cpp:87-105) with FP32 error bounds.
 __device__ __forceinline__ f3 offset_origin(f3 position, f3 geometric_normal, f3 position_error,
                                             f3 direction) {
     f3 normal = normalize(geometric_normal);
@@ -140,7 +140,7 @@ __device__ __forceinline__ f3 offset_origin(f3 position, f3 geometric_normal, f3
 
 // ---- frames and BSDFs (src/render/bsdf.cpp) ----
 
-struct Frame {  // ShadingFrame (bsdf.cpp:180-201)
+struct Frame {  // ShadingFrame (bsdf.cpp:89-110)
     f3 t, b, n;
     __device__ __forceinline__ void init(f3 normal) {
         const float maximum = fmaxf(fmaxf(fabsf(normal.x), fabsf(normal.y)), fabsf(normal.z));
@@ -153,13 +153,13 @@ struct Frame {  // ShadingFrame (bsdf.cpp:180-201)
     __device__ __forceinline__ f3 to_world(f3 l) const { return l.x * t + l.y * b + l.z * n; }
 };
 
-__device__ __forceinline__ float ggx_d(f3 m, float alpha) {  // bsdf.cpp:127-132
+__device__ __forceinline__ float ggx_d(f3 m, float alpha) {  // bsdf.cpp:36-41
     const float a2          = alpha * alpha;
     const float denominator = m.x * m.x + m.y * m.y + a2 * m.z * m.z;
     return m.z > 0 ? a2 / (kPi * denominator * denominator) : 0.0f;
 }
 
-__device__ __forceinline__ float smith_g1_over_cosine(f3 v, float alpha) {  // bsdf.cpp:134-139
+__device__ __forceinline__ float smith_g1_over_cosine(f3 v, float alpha) {  // bsdf.cpp:43-48
     if (v.z <= 0) {
         return 0.0f;
     }
@@ -167,7 +167,7 @@ __device__ __forceinline__ float smith_g1_over_cosine(f3 v, float alpha) {  // b
 }
 
 __device__ __forceinline__ float fresnel_from_transmission(float cosine, float sin2, float eta_i,
-                                                           float eta_t) {  // bsdf.cpp:142-155
+                                                           float eta_t) {  // bsdf.cpp:51-64
     if (eta_i == eta_t) {
         return 0.0f;
     }
@@ -180,14 +180,14 @@ __device__ __forceinline__ float fresnel_from_transmission(float cosine, float s
     return 0.5f * (parallel * parallel + perpendicular * perpendicular);
 }
 
-__device__ __forceinline__ f3 schlick(f3 f0, float cosine) {  // bsdf.cpp:157-160
+__device__ __forceinline__ f3 schlick(f3 f0, float cosine) {  // bsdf.cpp:66-69
     const float t  = 1.0f - fminf(fmaxf(cosine, 0.0f), 1.0f);
     const float t5 = t * t * t * t * t;
     return f0 + (make(1, 1, 1) - f0) * t5;
 }
 
 __device__ __forceinline__ f3 sample_visible_normal(f3 wo, float ux, float uy,
-                                                    float alpha) {  // bsdf.cpp:163-176
+                                                    float alpha) {  // bsdf.cpp:72-85
     const f3    view  = normalize(make(alpha * wo.x, alpha * wo.y, wo.z));
     const float lensq = view.x * view.x + view.y * view.y;
     const f3    t1    = lensq > 0 ? make(-view.y, view.x, 0) / sqrtf(lensq) : make(1, 0, 0);
@@ -202,7 +202,7 @@ __device__ __forceinline__ f3 sample_visible_normal(f3 wo, float ux, float uy,
     return normalize(make(alpha * normal.x, alpha * normal.y, fmaxf(0.0f, normal.z)));
 }
 
-struct Bsdf {  // Bsdf (bsdf.cpp:213-368) without cloth, subsurface and energy compensation
+struct Bsdf {  // Bsdf (bsdf.cpp:122-277) without cloth, subsurface and energy compensation
     f3       color;
     float    alpha, eta_i, eta_t;
     uint32_t kind;
@@ -304,7 +304,7 @@ struct Bsdf {  // Bsdf (bsdf.cpp:213-368) without cloth, subsurface and energy c
     }
 };
 
-__device__ __forceinline__ float power_heuristic(float sampled, float other) {  // path_tracer.cpp:206-218
+__device__ __forceinline__ float power_heuristic(float sampled, float other) {  // path_tracer.cpp:73-85
     const float scale = fmaxf(sampled, other);
     if (scale == 0) {
         return 0.0f;
@@ -317,7 +317,7 @@ __device__ __forceinline__ float power_heuristic(float sampled, float other) {  
 // ---- lights (src/render/light.cpp) ----
 
 __device__ __forceinline__ float area_density(f3 reference, f3 point, f3 normal,
-                                              float area) {  // light.cpp:192-200
+                                              float area) {  // light.cpp:49-57
     const f3    difference       = point - reference;
     const float squared_distance = dot(difference, difference);
     if (squared_distance == 0) {
@@ -334,7 +334,7 @@ struct LightSample {
     f3    position, normal, position_error;
 };
 
-// DiscreteDistribution::sample (sampling.cpp:210-220): upper_bound over the CDF.
+// DiscreteDistribution::sample (sampling.cpp:129-139): upper_bound over the CDF.
 __device__ __forceinline__ int select_light(const DeviceScene& s, float u, float& mass) {
     int lo = 0, hi = static_cast<int>(s.light_count) + 1;  // first cdf entry > u in [lo, hi)
     while (lo < hi) {
@@ -350,7 +350,7 @@ __device__ __forceinline__ int select_light(const DeviceScene& s, float u, float
     return index;
 }
 
-// LightSampler::sample (light.cpp:409-464), constant environment only.
+// LightSampler::sample (light.cpp:266-321), constant environment only.
 __device__ __forceinline__ bool sample_light(const DeviceScene& s, f3 reference, float light_u,
                                              float ux, float uy, LightSample& out) {
     if (s.light_count == 0) {
@@ -398,7 +398,7 @@ __device__ __forceinline__ bool sample_light(const DeviceScene& s, f3 reference,
     return true;
 }
 
-// LightSampler::area_pdf (light.cpp:466-477).
+// LightSampler::area_pdf (light.cpp:323-334).
 __device__ __forceinline__ float area_pdf(const DeviceScene& s, f3 reference, uint32_t prim,
                                           f3 position) {
     const uint32_t choice = __ldg(s.prim_emitter + prim);
@@ -413,7 +413,7 @@ __device__ __forceinline__ float area_pdf(const DeviceScene& s, f3 reference, ui
     return mass * area_density(reference, position, light.normal, light.area);
 }
 
-__device__ __forceinline__ float environment_pdf(const DeviceScene& s) {  // light.cpp:479-483
+__device__ __forceinline__ float environment_pdf(const DeviceScene& s) {  // light.cpp:336-340
     if (s.environment_choice < 0) {
         return 0.0f;
     }
@@ -422,7 +422,7 @@ __device__ __forceinline__ float environment_pdf(const DeviceScene& s) {  // lig
     return mass * (1.0f / (4.0f * kPi));
 }
 
-// The shadow segment of PathTracer::shadow_transmittance (path_tracer.cpp:259-284): both ends
+// The shadow segment of PathTracer::shadow_transmittance (path_tracer.cpp:126-151): both ends
 // offset by their error bounds, the far end pulled in by one ulp and 2^-18 of its length. Returns false when the
 // segment has zero length (the reference returns zero transmittance without tracing).
 __device__ __forceinline__ bool shadow_segment(f3 origin, const LightSample& light, f3& direction,

@@ -1,6 +1,6 @@
 // split.cu — early split clipping of oversized triangles before the binned-SAH build.
 //
-// The reference's builder (src/render/bvh.cpp:211-306) bins whole triangles by centroid. In a
+// The reference's builder (src/render/bvh.cpp:101-196) bins whole triangles by centroid. In a
 // scene of many small triangles and a few huge ones (the walls of a room around detailed
 // objects) the huge triangles' centroids fall among the small ones, so every node above a huge
 // triangle's leaf inherits its box, and rays test those large boxes again and again. Splitting

@@ -111,7 +111,7 @@ void carve(unsigned char* base, Workspace& ws, float4*& staging, unsigned*& inva
     }
 }
 
-// RayQuery / RayInterval validation (src/render/intersection.cpp:22-26,123-130) on the device,
+// RayQuery / RayInterval validation (src/render/intersection.cpp:22-26,52-61) on the device,
 // plus the copy into the wave's ray records. The unit-length check evaluates the squared length
 // in FP64 with the host check's operation order (validate_ray in abi.cu), so this entry point
 // rejects exactly the rays mr_trace_paths rejects; no path arithmetic uses FP64.
@@ -137,7 +137,7 @@ __global__ void stage_rays_kernel(const mr_ray* rays, uint32_t count, float4* st
     staging[2 * i + 1] = make_float4(r.direction[0], r.direction[1], r.direction[2], r.maximum);
 }
 
-// check_radiance (src/render/path_tracer.cpp:155-159) on the caller's output.
+// check_radiance (src/render/path_tracer.cpp:22-26) on the caller's output.
 __global__ void check_output_kernel(const float* radiance, uint32_t count, unsigned* error) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < 3 * count) {

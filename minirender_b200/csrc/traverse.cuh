@@ -1,7 +1,7 @@
 // traverse.cuh — FP32 ray queries over the BVH: slab test, watertight triangle test, nearest and
 // any-hit traversal.
 //
-// Semantics follow the reference exactly (src/render/intersection.cpp, src/render/bvh.cpp:316-410):
+// Semantics follow the reference exactly (src/render/intersection.cpp, src/render/bvh.cpp:206-300):
 // closed intervals, ties to the lower primitive id, single-sided culling by geometric winding,
 // any-hit exit on the first accepted triangle, pruning of popped subtrees whose entry distance
 // exceeds the current nearest hit. Differences are numeric only:
@@ -16,7 +16,7 @@
 namespace mr {
 
 // A wide node pushes <= 3 entries and sits at most 63 levels deep (built trees stop at 48,
-// bvh.cpp:126; imported trees are refused beyond 64 levels), so at most 3 * 63 entries are
+// bvh.cpp:16; imported trees are refused beyond 64 levels), so at most 3 * 63 entries are
 // stacked before any push: the check `sp > kStackSize - 3` never fires on an accepted tree.
 constexpr int      kStackSize  = 195;
 constexpr uint32_t kMaxVisits  = 1u << 16;  // node visits per ray before the query gives up
@@ -41,7 +41,7 @@ struct RayQuery {
             inv_hi[a] = inv * hi;
             neg[a]    = signbit(c);
         }
-        // Permutation and shear (src/render/intersection.cpp:130-145).
+        // Permutation and shear (src/render/intersection.cpp:62-74).
         const f3 ad = fabs3(d);
         kz          = ad.x > ad.y ? 0 : 1;
         if (ad.z > comp(ad, kz)) {
@@ -107,7 +107,7 @@ __device__ __forceinline__ void order2(float& ta, int& ra, float& tb, int& rb) {
 
 __device__ __forceinline__ float permuted(f3 v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
 
-// Watertight triangle test (src/render/intersection.cpp:179-223) in FP32. On acceptance returns
+// Watertight triangle test (src/render/intersection.cpp:108-152) in FP32. On acceptance returns
 // the distance and the three unnormalised edge functions plus their sum (the determinant).
 __device__ __forceinline__ bool triangle_test(const RayQuery& q, f3 v0, f3 v1, f3 v2, float tmin,
                                               float tmax, float& t, float& ea, float& eb,

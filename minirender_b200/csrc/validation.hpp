@@ -7,7 +7,7 @@
 
 namespace mr {
 
-// IntegratorSettings::validate (src/render/path_tracer.cpp:188-197).
+// IntegratorSettings::validate (src/render/path_tracer.cpp:55-64).
 inline IntegratorParams integrator_params(const mr_integrator_settings* s) {
     IntegratorParams p{MR_SAMPLING_MIS, 8, 1, 3};
     if (s) {
@@ -19,7 +19,7 @@ inline IntegratorParams integrator_params(const mr_integrator_settings* s) {
     return p;
 }
 
-// RenderSettings::validate (src/render/path_tracer.cpp:199-204).
+// RenderSettings::validate (src/render/path_tracer.cpp:66-71).
 inline void validate_render(const mr_render_settings* r) {
     require(r != nullptr, "Render settings are missing");
     if (r->width == 0 || r->height == 0 || r->width > 16384 || r->height > 16384 ||

@@ -8,7 +8,7 @@
 //           processed bin by bin so warps execute one material's code; appends the shadow
 //           queue and the next bounce's ray queue;
 //   shadow  any-hit traversal of the shadow queue, adding the unoccluded contributions.
-// The per-path logic is PathTracer::trace (src/render/path_tracer.cpp:286-499) in FP32 with the
+// The per-path logic is PathTracer::trace (src/render/path_tracer.cpp:153-366) in FP32 with the
 // reference's RNG stream layout; every path writes only its own state, so images do not depend
 // on scheduling. Radiance is kept per path and added to the pixels in sample order after the
 // wave (compensated FP32 sums), so a frame is deterministic.
@@ -122,7 +122,7 @@ __device__ __forceinline__ void init_path(const KernelArgs& a, uint32_t slot, Pc
 }
 
 // Stream derivation, film jitter and lens sample of one camera sample (PathTracer::sample_pixel,
-// src/render/path_tracer.cpp:501-519).
+// src/render/path_tracer.cpp:368-386).
 __device__ __forceinline__ CameraRay camera_sample(const CameraBasis& camera, uint32_t x, uint32_t y,
                                                    uint64_t sample, uint32_t width, uint32_t height,
                                                    uint64_t seed, Pcg32& rng) {
@@ -260,7 +260,7 @@ __device__ __forceinline__ uint32_t extend_item(const KernelArgs& a, const Devic
     uint32_t key        = r.slot == kNone ? kBinMiss : kBinDiffuse + kind;
     if (MEDIA && s.medium_count > 0) {
         // MediumField::sample over [minimum, hit ? distance : maximum]
-        // (src/render/path_tracer.cpp:303-310).
+        // (src/render/path_tracer.cpp:170-177).
         Pcg32  rng   = load_rng(a.st, path);
         float4 beta4 = a.st.beta[path];
         bool   scattered;
@@ -375,7 +375,7 @@ __device__ __forceinline__ float emission_weight(const IntegratorParams& p, uint
     return p.mode == MR_SAMPLING_MIS ? power_heuristic(previous_pdf, light_pdf) : 0.0f;
 }
 
-// Russian roulette (src/render/path_tracer.cpp:485-495). Returns false when the path ends.
+// Russian roulette (src/render/path_tracer.cpp:352-362). Returns false when the path ends.
 __device__ __forceinline__ bool roulette(const IntegratorParams& p, uint32_t depth, Pcg32& rng,
                                          f3& beta, float eta_scale, uint32_t& rr_count) {
     const float u = rng.next_1d();
@@ -420,7 +420,7 @@ __device__ ShadeResult shade_surface(const KernelArgs& a, uint32_t path, int bin
     }
     Pcg32 rng = load_rng(a.st, path);
     if (bin == kBinMedium) {
-        // Medium vertex (src/render/path_tracer.cpp:311-356).
+        // Medium vertex (src/render/path_tracer.cpp:178-223).
         const float4 h      = a.st.hit[path];
         const float4 o4     = a.st.ray_o[path];
         const f3     vertex = xyz(o4) + h.x * dir;
@@ -470,7 +470,7 @@ __device__ ShadeResult shade_surface(const KernelArgs& a, uint32_t path, int bin
         return out;
     }
 
-    // Surface vertex (src/render/path_tracer.cpp:357-496).
+    // Surface vertex (src/render/path_tracer.cpp:224-363).
     const float4     h   = a.st.hit[path];
     const uint32_t   slot = a.st.hit_slot[path];
     const SurfaceHit sh  = surface_hit(s, dir, slot, h.y, h.z, h.w);
@@ -616,7 +616,7 @@ __device__ __forceinline__ void neumaier(float& sum, float& comp, float v) {
 }
 
 // Adds the wave's per-path radiance to the pixels in sample order; checks every path result
-// like check_radiance (src/render/path_tracer.cpp:155-159).
+// like check_radiance (src/render/path_tracer.cpp:22-26).
 __global__ void resolve_kernel(const float4* radiance, uint32_t x0, uint32_t y0, uint32_t w,
                                uint32_t h, uint32_t ns, uint32_t width, float4* accumulator,
                                uint32_t accumulator_row0, unsigned* error) {
@@ -695,7 +695,7 @@ __global__ void __launch_bounds__(256) resolve_batch_kernel(const float4* radian
     }
 }
 
-// Pixel mean and the overflow check of PathTracer::render (src/render/path_tracer.cpp:527-534).
+// Pixel mean and the overflow check of PathTracer::render (src/render/path_tracer.cpp:394-401).
 __global__ void finalize_kernel(const float4* accumulator, size_t pixels, uint32_t spp, float* rgb,
                                 unsigned* error) {
     const size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;

@@ -148,7 +148,7 @@ def trace_normals(scene_path: str, output: str) -> int:
     cosine = d @ forward
     hits, counters = scene.intersect(np.broadcast_to(position, d.shape), d,
                                      c.near_plane / cosine, c.far_plane / cosine)
-    # SceneBvh::surface_hit's shading normal (src/render/bvh.cpp:412-440): barycentric sum of
+    # SceneBvh::surface_hit's shading normal (src/render/bvh.cpp:302-330): barycentric sum of
     # the unit world corner normals, oriented to the geometric normal's side.
     visible = [o for o in doc.objects if o.visible]
     image = np.zeros((size * size, 3), f32)

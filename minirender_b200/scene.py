@@ -276,7 +276,7 @@ class Snapshot:
 
     def world_triangles(self) -> np.ndarray:
         """World-space float32 vertices (N, 3, 3) in primitive order, computed like
-        SceneBvh's constructor (src/render/bvh.cpp:163-199)."""
+        SceneBvh's constructor (src/render/bvh.cpp:53-89)."""
         out = []
         for o, (m, _) in zip([o for o in self.document.objects if o.visible], self.matrices):
             mesh = self.document.meshes[o.mesh]

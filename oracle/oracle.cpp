@@ -91,7 +91,7 @@ void require(bool condition, const char* message) {
 
 // ---- sampling (src/core/sampling.cpp) ----------------------------------------------------
 
-void check_unit(double u) {  // sampling.cpp:97-101
+void check_unit(double u) {  // sampling.cpp:16-20
     if (!(u >= 0 && u < 1)) {
         throw std::invalid_argument("Sample coordinate must be in [0,1)");
     }
@@ -101,13 +101,13 @@ void check_unit(dvec2 u) {
     check_unit(u.y);
 }
 
-std::uint64_t mix(std::uint64_t value) {  // sampling.cpp:109-113 (SplitMix64 finaliser)
+std::uint64_t mix(std::uint64_t value) {  // sampling.cpp:28-32 (SplitMix64 finaliser)
     value = (value ^ (value >> 30U)) * 0xbf58476d1ce4e5b9ULL;
     value = (value ^ (value >> 27U)) * 0x94d049bb133111ebULL;
     return value ^ (value >> 31U);
 }
 
-class Sampler {  // sampling.cpp:117-146, PCG32 XSH-RR
+class Sampler {  // sampling.cpp:36-65, PCG32 XSH-RR
   public:
     explicit Sampler(std::uint64_t seed = 0, std::uint64_t sequence = 1)
         : increment_((sequence << 1U) | 1U) {
@@ -143,7 +143,7 @@ class Sampler {  // sampling.cpp:117-146, PCG32 XSH-RR
     std::uint64_t increment_ = 1;
 };
 
-dvec2 sample_disk(dvec2 u) {  // sampling.cpp:148-160, Shirley-Chiu concentric map
+dvec2 sample_disk(dvec2 u) {  // sampling.cpp:67-79, Shirley-Chiu concentric map
     check_unit(u);
     const dvec2 square{2.0 * u.x - 1.0, 2.0 * u.y - 1.0};
     if (square.x == 0 && square.y == 0) {
@@ -156,31 +156,31 @@ dvec2 sample_disk(dvec2 u) {  // sampling.cpp:148-160, Shirley-Chiu concentric m
     return {radius * std::cos(angle), radius * std::sin(angle)};
 }
 
-dvec3 sample_sphere(dvec2 u) {  // sampling.cpp:162-167
+dvec3 sample_sphere(dvec2 u) {  // sampling.cpp:81-86
     check_unit(u);
     const double z      = 1 - 2 * u.x;
     const double radius = std::sqrt(std::max(0.0, 1 - z * z));
     return {radius * std::cos(2 * pi * u.y), radius * std::sin(2 * pi * u.y), z};
 }
 
-dvec3 sample_hemisphere(dvec2 u) {  // sampling.cpp:169-173
+dvec3 sample_hemisphere(dvec2 u) {  // sampling.cpp:88-92
     check_unit(u);
     const double radius = std::sqrt(std::max(0.0, 1 - u.x * u.x));
     return {radius * std::cos(2 * pi * u.y), radius * std::sin(2 * pi * u.y), u.x};
 }
 
-dvec3 sample_cosine_hemisphere(dvec2 u) {  // sampling.cpp:175-178
+dvec3 sample_cosine_hemisphere(dvec2 u) {  // sampling.cpp:94-97
     const auto disk = sample_disk(u);
     return {disk.x, disk.y, std::sqrt(std::max(0.0, 1 - dot2(disk, disk)))};
 }
 
-dvec3 sample_triangle(dvec2 u) {  // sampling.cpp:180-184
+dvec3 sample_triangle(dvec2 u) {  // sampling.cpp:99-103
     check_unit(u);
     const double root = std::sqrt(u.x);
     return {1 - root, root * (1 - u.y), root * u.y};
 }
 
-double cosine_hemisphere_pdf(dvec3 direction) {  // sampling.cpp:186-188
+double cosine_hemisphere_pdf(dvec3 direction) {  // sampling.cpp:105-107
     return std::max(0.0, direction.z) / pi;
 }
 
@@ -190,7 +190,7 @@ struct DiscreteSample {
     double      remapped    = 0;
 };
 
-class DiscreteDistribution {  // sampling.cpp:190-231
+class DiscreteDistribution {  // sampling.cpp:109-150
   public:
     DiscreteDistribution() : cdf_(1, 0) {}
     explicit DiscreteDistribution(const std::vector<double>& weights)
@@ -445,7 +445,7 @@ struct Snapshot {
     std::vector<MediumRegion>         media;
 };
 
-// glm::vec3(object_to_world * glm::vec4(p, 1)) in float (bvh.cpp:178-179).
+// glm::vec3(object_to_world * glm::vec4(p, 1)) in float (bvh.cpp:68-69).
 fvec3 transform_point(const float* m, fvec3 p) {
     fvec3 r;
     for (int row = 0; row < 3; ++row) {
@@ -458,7 +458,7 @@ fvec3 transform_point(const float* m, fvec3 p) {
     return r;
 }
 
-// glm::determinant(glm::dmat3(object_to_world)) (bvh.cpp:166).
+// glm::determinant(glm::dmat3(object_to_world)) (bvh.cpp:56).
 double determinant3(const float* m) {
     const auto e = [m](int c, int r) { return static_cast<double>(m[4 * c + r]); };
     return +e(0, 0) * (e(1, 1) * e(2, 2) - e(2, 1) * e(1, 2)) -
@@ -466,7 +466,7 @@ double determinant3(const float* m) {
            e(2, 0) * (e(0, 1) * e(1, 2) - e(1, 1) * e(0, 2));
 }
 
-// glm::dmat3(normal_to_world) * dvec3(n) (bvh.cpp:429-430).
+// glm::dmat3(normal_to_world) * dvec3(n) (bvh.cpp:319-320).
 dvec3 transform_normal(const float* m, fvec3 n) {
     dvec3 r;
     for (int row = 0; row < 3; ++row) {
@@ -592,10 +592,10 @@ std::shared_ptr<Snapshot> make_snapshot(const mr_scene_desc& d) {
 
 // ---- BVH (src/render/bvh.cpp) ------------------------------------------------------------
 
-constexpr std::uint32_t bin_count           = 12;  // bvh.cpp:125
-constexpr std::size_t   maximum_build_depth = 48;  // bvh.cpp:126
+constexpr std::uint32_t bin_count           = 12;  // bvh.cpp:15
+constexpr std::size_t   maximum_build_depth = 48;  // bvh.cpp:16
 
-std::uint32_t bin_index(float centroid, float low, float high) {  // bvh.cpp:133-137
+std::uint32_t bin_index(float centroid, float low, float high) {  // bvh.cpp:23-27
     const double coordinate =
         (static_cast<double>(centroid) - low) / (static_cast<double>(high) - low);
     return std::min(static_cast<std::uint32_t>(coordinate * bin_count), bin_count - 1);
@@ -643,7 +643,7 @@ class SceneBvh {
         TriangleHit   hit;
     };
 
-    // bvh.cpp:141-209 (world-space flattening + build); `imported` replaces the build.
+    // bvh.cpp:31-99 (world-space flattening + build); `imported` replaces the build.
     SceneBvh(std::shared_ptr<const Snapshot> scene, const mr_bvh_desc* imported = nullptr)
         : scene_(std::move(scene)) {
         std::size_t total = 0;
@@ -720,7 +720,7 @@ class SceneBvh {
         }
     }
 
-    // bvh.cpp:211-306, recursive 12-bin SAH build in DFS pre-order.
+    // bvh.cpp:101-196, recursive 12-bin SAH build in DFS pre-order.
     std::uint32_t build(std::uint32_t begin, std::uint32_t end, std::size_t depth,
                         const std::vector<BuildPrimitive>& primitives) {
         const auto node_index = static_cast<std::uint32_t>(nodes_.size());
@@ -807,7 +807,7 @@ class SceneBvh {
         return node_index;
     }
 
-    // bvh.cpp:316-410, ordered DFS with closed intervals and the lower-id tie rule.
+    // bvh.cpp:206-300, ordered DFS with closed intervals and the lower-id tie rule.
     std::optional<PrimitiveHit> trace(const Ray& ray, RayInterval interval, bool any_hit,
                                       TraceStatistics* statistics) const {
         interval.validate();
@@ -890,7 +890,7 @@ class SceneBvh {
         return result;
     }
 
-    // bvh.cpp:412-480 without normal maps (the configs have none).
+    // bvh.cpp:302-370 without normal maps (the configs have none).
     SurfaceHit surface_hit(const Ray& ray, const PrimitiveHit& hit) const {
         const auto& primitive = primitives_[hit.primitive];
         const auto& instance  = scene_->instances[primitive.instance];
@@ -941,7 +941,7 @@ class SceneBvh {
         return trace(ray, interval, true, statistics).has_value();
     }
 
-    // Whole-tree SAH cost with C_T = C_I = 1 (the constants of bvh.cpp:244-245).
+    // Whole-tree SAH cost with C_T = C_I = 1 (the constants of bvh.cpp:134-135).
     double sah_cost() const {
         if (nodes_.empty()) {
             return 0;
@@ -971,28 +971,28 @@ class SceneBvh {
 
 // ---- BSDF (src/render/bsdf.cpp) -----------------------------------------------------------
 
-constexpr double delta_alpha = 1e-6;  // bsdf.cpp:108
+constexpr double delta_alpha = 1e-6;  // bsdf.cpp:17
 
-dvec3 unit_direction(dvec3 value) {  // bsdf.cpp:114-119
+dvec3 unit_direction(dvec3 value) {  // bsdf.cpp:23-28
     if (!finite3(value) || std::abs(dot(value, value) - 1) > 1e-4) {
         throw std::invalid_argument("BSDF direction must be finite and have unit length");
     }
     return normalize(value);
 }
 
-void check_bsdf_sample(double value) {  // bsdf.cpp:121-125
+void check_bsdf_sample(double value) {  // bsdf.cpp:30-34
     if (!(value >= 0 && value < 1)) {
         throw std::invalid_argument("BSDF sample coordinate must be in [0,1)");
     }
 }
 
-double distribution(dvec3 m, double alpha) {  // bsdf.cpp:127-132, GGX D
+double distribution(dvec3 m, double alpha) {  // bsdf.cpp:36-41, GGX D
     const double a2          = alpha * alpha;
     const double denominator = m.x * m.x + m.y * m.y + a2 * m.z * m.z;
     return m.z > 0 ? a2 / (pi * denominator * denominator) : 0;
 }
 
-double smith_g1_over_cosine(dvec3 v, double alpha) {  // bsdf.cpp:134-139
+double smith_g1_over_cosine(dvec3 v, double alpha) {  // bsdf.cpp:43-48
     if (v.z <= 0) {
         return 0;
     }
@@ -1000,7 +1000,7 @@ double smith_g1_over_cosine(dvec3 v, double alpha) {  // bsdf.cpp:134-139
 }
 
 double fresnel_from_transmission(double cosine, double sin2, double eta_i,
-                                 double eta_t) {  // bsdf.cpp:142-155
+                                 double eta_t) {  // bsdf.cpp:51-64
     if (eta_i == eta_t) {
         return 0;
     }
@@ -1015,13 +1015,13 @@ double fresnel_from_transmission(double cosine, double sin2, double eta_i,
     return 0.5 * (parallel * parallel + perpendicular * perpendicular);
 }
 
-dvec3 schlick(dvec3 f0, double cosine) {  // bsdf.cpp:157-160
+dvec3 schlick(dvec3 f0, double cosine) {  // bsdf.cpp:66-69
     const double t  = 1 - std::clamp(cosine, 0.0, 1.0);
     const double t5 = t * t * t * t * t;
     return f0 + (dvec3{1, 1, 1} - f0) * t5;
 }
 
-dvec3 sample_visible_normal(dvec3 wo, dvec2 u, double alpha) {  // bsdf.cpp:163-176, Heitz 2018
+dvec3 sample_visible_normal(dvec3 wo, dvec2 u, double alpha) {  // bsdf.cpp:72-85, Heitz 2018
     const auto   view  = normalize(dvec3{alpha * wo.x, alpha * wo.y, wo.z});
     const double lensq = view.x * view.x + view.y * view.y;
     const auto t1 = lensq > 0 ? dvec3{-view.y, view.x, 0} / std::sqrt(lensq) : dvec3{1, 0, 0};
@@ -1035,7 +1035,7 @@ dvec3 sample_visible_normal(dvec3 wo, dvec2 u, double alpha) {  // bsdf.cpp:163-
     return normalize(dvec3{alpha * normal.x, alpha * normal.y, std::max(0.0, normal.z)});
 }
 
-class ShadingFrame {  // bsdf.cpp:180-201
+class ShadingFrame {  // bsdf.cpp:89-110
   public:
     explicit ShadingFrame(dvec3 normal) {
         const double maximum = std::max({std::abs(normal.x), std::abs(normal.y), std::abs(normal.z)});
@@ -1055,7 +1055,7 @@ class ShadingFrame {  // bsdf.cpp:180-201
     dvec3 tangent_, bitangent_, normal_;
 };
 
-double fresnel_dielectric(double cosine, double eta_i, double eta_t) {  // bsdf.cpp:203-211
+double fresnel_dielectric(double cosine, double eta_i, double eta_t) {  // bsdf.cpp:112-120
     if (!std::isfinite(cosine) || cosine < 0 || cosine > 1 || !std::isfinite(eta_i) ||
         !std::isfinite(eta_t) || eta_i <= 0 || eta_t <= 0) {
         throw std::invalid_argument("Fresnel requires cosine in [0,1] and positive finite IORs");
@@ -1076,7 +1076,7 @@ struct BsdfSample {
     double eta         = 1;
 };
 
-class Bsdf {  // bsdf.cpp:213-368 without cloth and energy compensation
+class Bsdf {  // bsdf.cpp:122-277 without cloth and energy compensation
   public:
     Bsdf(const Material& material, bool front_face, bool importance = false)
         : kind_(material.kind), color_(widen(material.base_color)),
@@ -1167,11 +1167,11 @@ class Bsdf {  // bsdf.cpp:213-368 without cloth and energy compensation
 
 // ---- lights (src/render/light.cpp) --------------------------------------------------------
 
-double luminance(dvec3 c) {  // light.cpp:164-166
+double luminance(dvec3 c) {  // light.cpp:21-23
     return dot(c, dvec3{0.2126, 0.7152, 0.0722});
 }
 
-double area_density(dvec3 reference, dvec3 point, dvec3 normal, double area) {  // light.cpp:192-200
+double area_density(dvec3 reference, dvec3 point, dvec3 normal, double area) {  // light.cpp:49-57
     const auto   difference       = point - reference;
     const double squared_distance = dot(difference, difference);
     if (squared_distance == 0) {
@@ -1194,10 +1194,10 @@ struct LightSample {
     dvec3       position, normal, position_error;
 };
 
-class LightSampler {  // light.cpp:204-497, constant environment only
+class LightSampler {  // light.cpp:61-354, constant environment only
   public:
     explicit LightSampler(const Snapshot& scene) : constant_(widen(scene.environment)) {
-        integral_ = 4 * pi * luminance(constant_);  // light.cpp:209
+        integral_ = 4 * pi * luminance(constant_);  // light.cpp:66
         Bounds3             bounds;
         std::vector<double> weights;
         for (std::size_t index = 0; index < scene.instances.size(); ++index) {
@@ -1252,8 +1252,8 @@ class LightSampler {  // light.cpp:204-497, constant environment only
         selection_ = DiscreteDistribution(weights);
     }
 
-    dvec3  environment_evaluate(dvec3) const { return constant_; }           // light.cpp:283-286
-    double environment_density(dvec3) const { return 1 / (4 * pi); }        // light.cpp:288-291
+    dvec3  environment_evaluate(dvec3) const { return constant_; }           // light.cpp:140-143
+    double environment_density(dvec3) const { return 1 / (4 * pi); }        // light.cpp:145-148
 
     std::optional<LightSample> sample(dvec3 reference, double light_u, dvec2 surface_u) const {
         if (!finite3(reference)) {
@@ -1277,7 +1277,7 @@ class LightSampler {  // light.cpp:204-497, constant environment only
             return s;
         }
         if (choice.kind == LightKind::environment) {
-            const auto  direction = sample_sphere({surface_u.x, surface_u.y});  // light.cpp:305-306
+            const auto  direction = sample_sphere({surface_u.x, surface_u.y});  // light.cpp:162-163
             LightSample s;
             s.direction   = direction;
             s.radiance    = environment_evaluate(direction);
@@ -1315,7 +1315,7 @@ class LightSampler {  // light.cpp:204-497, constant environment only
         return s;
     }
 
-    double area_pdf(dvec3 reference, const SurfaceHit& hit) const {  // light.cpp:466-477
+    double area_pdf(dvec3 reference, const SurfaceHit& hit) const {  // light.cpp:323-334
         const auto choice = area_choices_.find({hit.instance_index, hit.triangle_index});
         if (choice == area_choices_.end()) {
             return 0;
@@ -1328,7 +1328,7 @@ class LightSampler {  // light.cpp:204-497, constant environment only
                area_density(reference, hit.position, light.normal, light.area);
     }
 
-    double environment_pdf(dvec3 direction) const {  // light.cpp:479-483
+    double environment_pdf(dvec3 direction) const {  // light.cpp:336-340
         return environment_choice_
                    ? selection_.probability(*environment_choice_) * environment_density(direction)
                    : 0;
@@ -1567,7 +1567,7 @@ struct IntegratorSettings {
     std::uint32_t maximum_depth  = 8;
     bool          russian_roulette = true;
     std::uint32_t roulette_depth = 3;
-    void          validate() const {  // path_tracer.cpp:188-197
+    void          validate() const {  // path_tracer.cpp:55-64
         require(mode <= MR_SAMPLING_MIS, "Sampling mode must be bsdf, light or mis");
         require(maximum_depth <= 128 && roulette_depth <= 128,
                 "Path and roulette depths must not exceed 128");
@@ -1578,7 +1578,7 @@ struct RenderSettings {
     std::size_t   width = 256, height = 256;
     std::uint32_t samples_per_pixel = 64;
     std::uint64_t seed              = 1;
-    void          validate() const {  // path_tracer.cpp:199-204
+    void          validate() const {  // path_tracer.cpp:66-71
         if (width == 0 || height == 0 || width > 16384 || height > 16384 ||
             width * height > 64U * 1024U * 1024U || samples_per_pixel == 0) {
             throw std::invalid_argument("Render dimensions or sample count exceed the image budget");
@@ -1601,13 +1601,13 @@ struct PathStatistics {
     }
 };
 
-void check_radiance(dvec3 value) {  // path_tracer.cpp:155-159
+void check_radiance(dvec3 value) {  // path_tracer.cpp:22-26
     if (!finite3(value) || value.x < 0 || value.y < 0 || value.z < 0) {
         throw std::runtime_error("Path contribution is nonfinite or negative");
     }
 }
 
-double power_heuristic(double sampled_pdf, double other_pdf) {  // path_tracer.cpp:206-218
+double power_heuristic(double sampled_pdf, double other_pdf) {  // path_tracer.cpp:73-85
     if (!std::isfinite(sampled_pdf) || !std::isfinite(other_pdf) || sampled_pdf < 0 ||
         other_pdf < 0) {
         throw std::invalid_argument("MIS probabilities must be finite and nonnegative");
@@ -1622,7 +1622,7 @@ double power_heuristic(double sampled_pdf, double other_pdf) {  // path_tracer.c
 }
 
 dvec3 offset_origin(dvec3 position, fvec3 geometric_normal, dvec3 position_error,
-                    dvec3 direction) {  // path_tracer.cpp:220-238
+                    dvec3 direction) {  // path_tracer.cpp:87-105
     auto normal = normalize(widen(geometric_normal));
     if (dot(normal, direction) < 0) {
         normal = -normal;
@@ -1639,7 +1639,7 @@ dvec3 offset_origin(dvec3 position, fvec3 geometric_normal, dvec3 position_error
     return origin;
 }
 
-Ray spawn_ray(const SurfaceHit& hit, dvec3 direction) {  // path_tracer.cpp:240-242
+Ray spawn_ray(const SurfaceHit& hit, dvec3 direction) {  // path_tracer.cpp:107-109
     return {offset_origin(hit.position, hit.geometric_normal, hit.position_error, direction),
             normalize(direction)};
 }
@@ -1653,7 +1653,7 @@ class PathTracer {
         settings_.validate();
     }
 
-    // path_tracer.cpp:259-284
+    // path_tracer.cpp:126-151
     dvec3 shadow_transmittance(Ray ray, const LightSample& light, PathStatistics* statistics) const {
         if (statistics) {
             ++statistics->shadow_rays;
@@ -1676,7 +1676,7 @@ class PathTracer {
         return media_.transmittance(ray, {0, limit});
     }
 
-    // path_tracer.cpp:286-499 (subsurface branch omitted: the material is rejected).
+    // path_tracer.cpp:153-366 (subsurface branch omitted: the material is rejected).
     dvec3 trace(Ray ray, Sampler& sampler, RayInterval primary_interval,
                 PathStatistics* statistics) const {
         if (statistics) {
@@ -1833,7 +1833,7 @@ class PathTracer {
         return result;
     }
 
-    // path_tracer.cpp:501-519 (also returns the camera ray and its interval).
+    // path_tracer.cpp:368-386 (also returns the camera ray and its interval).
     dvec3 sample_pixel(std::size_t x, std::size_t y, std::uint64_t sample_index,
                        const RenderSettings& settings, PathStatistics* statistics,
                        Ray* ray_out = nullptr, RayInterval* interval_out = nullptr) const {
@@ -1902,7 +1902,7 @@ class PathTracer {
 
 // Tile-parallel render with the accumulation order of RenderSession (render_session.cpp:386-459):
 // each pixel's samples are summed in sample order in double, so the image is bitwise identical
-// to the serial PathTracer::render (path_tracer.cpp:521-538) for any thread count.
+// to the serial PathTracer::render (path_tracer.cpp:388-405) for any thread count.
 void render_rows(const PathTracer& tracer, const RenderSettings& settings, std::size_t row_begin,
                  std::size_t row_end, unsigned threads, float* rgb, PathStatistics* statistics) {
     settings.validate();
@@ -2488,7 +2488,7 @@ int or_area_pdf_at_hit(void* scene, const double* reference, const DRay* ray, do
 }
 
 int or_display_image(const float* linear, uint64_t width, uint64_t height, double exposure,
-                     float* display) {  // path_tracer.cpp:540-557
+                     float* display) {  // path_tracer.cpp:407-424
     return guarded([&] {
         if (!std::isfinite(exposure) || std::abs(exposure) > 64) {
             throw std::invalid_argument("Display exposure must be finite and in [-64,64]");

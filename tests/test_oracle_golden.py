@@ -414,7 +414,7 @@ def floor_doc(kind="diffuse", color=0.6):
 
 
 def direct_doc(glossy):
-    """tests/path_tests.cpp:54-66"""
+    """tests/path_tests.cpp:56-67"""
     doc = floor_doc("conductor" if glossy else "diffuse", 0.8 if glossy else 0.7)
     doc.environment = (0.0, 0.0, 0.0)
     doc.materials[0].roughness = 0.15
@@ -437,7 +437,7 @@ def estimate(o, count, seed, origin=(0, 1, 0), direction=(0, -1, 0), interval=(0
 
 
 def sampler_doubles(oracle, seed, count, sequence=1):
-    """Sampler(seed, sequence).next_1d() values (src/core/sampling.cpp:137-141)."""
+    """Sampler(seed, sequence).next_1d() values (src/core/sampling.cpp:56-60)."""
     raw = oracle.pcg_sequence(seed, sequence, 2 * count).astype(np.uint64)
     hi = raw[0::2] >> np.uint64(5)
     lo = raw[1::2] >> np.uint64(6)
