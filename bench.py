@@ -76,6 +76,10 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-serve", action="store_true")
+    p.add_argument("--serve-rate", type=float, default=SERVE_RATE,
+                   help="Poisson arrival rate of the serving run, jobs per second")
+    p.add_argument("--leg", choices=["serve", "stress"], default=None,
+                   help="run one secondary workload alone and print its JSON line")
     p.add_argument("--stress", action="store_true",
                    help="also render the 20M-triangle scene in a medium at 3840x2160, 256 spp, "
                         "depth 16 (about half a minute)")
@@ -538,6 +542,59 @@ def config1_leg(api, sc, stream, with_cpu):
     return out
 
 
+def stress_leg(api, sc, stream):
+    """Config 5: 4,000 displaced icospheres (20.48M triangles) in one homogeneous medium,
+    3840x2160, 256 spp, depth 16, after a 960x540x4 warm-up frame."""
+    import torch
+    doc = sc.stress_scene()
+    t0 = time.perf_counter()
+    big = api.Scene(doc.snapshot())
+    torch.cuda.synchronize()
+    build_s = time.perf_counter() - t0
+    tracer = api.PathTracer(big, api.IntegratorSettings("mis", 16, True, 3))
+    out = torch.empty(3840 * 2160 * 3, dtype=torch.float32, device="cuda")
+    full = api.RenderSettings(3840, 2160, 256, 1)
+    tracer.render_device(api.RenderSettings(960, 540, 4, 1), out.data_ptr(), stream.cuda_stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    tracer.render_device(full, out.data_ptr(), stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    result = {"workload": "4000 displaced icospheres (20.48M triangles) in one homogeneous "
+                          "medium, 3840x2160, 256 spp, depth 16, reference builder",
+              "ms": ms, "value": 3840 * 2160 * 256 / ms / 1e3, "unit": METRIC,
+              "scene_create_s": build_s, "bvh_build_ms": 1e3 * big.build_seconds(),
+              "triangles": doc.triangle_count}
+    big.close()
+    return result
+
+
+def run_leg(args):
+    """One secondary workload alone, for a recorded profile: `serve` (the Poisson request stream
+    through the render server over --serve-seconds at --serve-rate jobs/s) or `stress`
+    (config 5). Prints one JSON line with the clocks seen meanwhile."""
+    import torch
+    from minirender_b200 import api
+    from minirender_b200 import scene as sc
+    torch.cuda.set_device(0)
+    stream = torch.cuda.current_stream()
+    clocks = ClockSampler(0)
+    if args.leg == "serve":
+        table = job_table(args.jobs)
+        scenes = [api.Scene(job_document(j).snapshot(), split_references=True) for j in table]
+        torch.cuda.synchronize()
+        clocks.start()
+        result = serve(api, scenes, table, args.serve_seconds, np.random.default_rng(50),
+                       args.serve_rate)
+    else:
+        clocks.start()
+        result = stress_leg(api, sc, stream)
+    print(json.dumps({"leg": args.leg, "command": "python bench.py " + " ".join(sys.argv[1:]),
+                      **result, "clocks": clocks.stop()}), flush=True)
+    return 0
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -733,27 +790,7 @@ def run_ours(args):
         sustainable = serve(api, scenes, table, args.serve_seconds, np.random.default_rng(16),
                             SUSTAINABLE_RATE)
 
-    stress = None
-    if args.stress:
-        doc = sc.stress_scene()
-        t0 = time.perf_counter()
-        big = api.Scene(doc.snapshot())
-        torch.cuda.synchronize()
-        build_s = time.perf_counter() - t0
-        tracer = api.PathTracer(big, api.IntegratorSettings("mis", 16, True, 3))
-        out = torch.empty(3840 * 2160 * 3, dtype=torch.float32, device="cuda")
-        tracer.render_device(api.RenderSettings(960, 540, 4, 1), out.data_ptr(), stream.cuda_stream)
-        full = api.RenderSettings(3840, 2160, 256, 1 + rank)
-        e0.record(stream)
-        tracer.render_device(full, out.data_ptr(), stream.cuda_stream)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1)
-        stress = {"workload": "4000 displaced icospheres (20.48M triangles) in one homogeneous "
-                              "medium, 3840x2160, 256 spp, depth 16, reference builder",
-                  "ms": ms, "value": 3840 * 2160 * 256 / ms / 1e3, "unit": METRIC,
-                  "scene_create_s": build_s, "bvh_build_ms": 1e3 * big.build_seconds()}
-        big.close()
+    stress = stress_leg(api, sc, stream) if args.stress and world == 1 else None
 
     peak, peak_kind = measured_peak()
     algorithmic = (BYTES_PER_BOUNDS_TEST * counted.bounds_tests +
@@ -861,6 +898,8 @@ def main():
         return trace_sample(args.trace_sample)
     if args.impl == "reference":
         return run_reference(args)
+    if args.leg:
+        return run_leg(args)
     return run_ours(args)
 
 

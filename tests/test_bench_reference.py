@@ -23,3 +23,11 @@ def test_reference_arm_prints_the_contract_line():
     assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] >= 1
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["value"] == line["value"]
     assert "workload" in line["config"]
+    # The workload description is the one the GPU arm prints: the job scenes' exact triangles.
+    sys.path.insert(0, ROOT)
+    import bench
+    from minirender_b200 import scene as sc
+    table = sc.job_table(256, bench.TABLE_SEED)[:8]
+    assert line["config"] == bench.config(table)
+    assert line["config"]["triangles_total"] == sum(
+        sc.job_scene_triangles(j["triangles"]) for j in table)

@@ -1,5 +1,6 @@
 """bench.py's own arm on the GPU prints one JSON line with the contract's keys: run on four jobs
-of the mix with the default wave shape, one timed step, no serving, e2e or CPU legs."""
+of the mix with the default wave shape, one timed step, no serving, e2e or CPU legs. The
+secondary legs (per-quintile batched vs plain, config 1, the 1080p frame) report."""
 
 import json
 import os
@@ -41,3 +42,8 @@ def test_bench_prints_the_contract_line():
     preview = line["config"]["preview_jobs"]
     assert "error" not in preview, preview
     assert preview["batched"] > 0 and preview["plain"] > 0
+    assert all(q["batched_vs_plain"] > 0 for q in line["config"]["quintiles"])
+    c1 = line["config"]["config1"]
+    assert c1["value"] > 0 and c1["e2e"]["value"] > 0
+    assert line["config"]["large_frame"]["value"] > 0
+    assert line["roofline"]["dram"]["achieved"] is None or line["roofline"]["dram"]["achieved"] > 0
