@@ -300,15 +300,46 @@ typedef struct mr_build_settings {
                                   slots differ from the reference builder's. */
     float    split_factor;     /* 0 = 16 */
     uint64_t max_references;   /* cap on leaf slots; 0 = max(2 x triangles, triangles + 65536) */
+    uint32_t two_level;        /* nonzero: an instance-level tree (TLAS) over one object-space
+                                  tree per mesh (BLAS) instead of the reference's flattened
+                                  world-space tree (src/render/bvh.cpp:31-99). Triangles are still
+                                  tested in world space with the flattening's own arithmetic, so
+                                  hits, images and path statistics other than the traversal
+                                  counters equal the flattened scene's; a mesh instanced many
+                                  times is stored once. Not combinable with split references or
+                                  an imported tree. Enables mr_scene_update_instances and
+                                  mr_scene_update_mesh. */
 } mr_build_settings;
 
 /* mr_scene_create with builder options (`build` NULL = mr_scene_create). A scene built with
- * split references cannot be exported in the reference layout (MR_LOGIC_ERROR). */
+ * split references or two levels cannot be exported in the reference layout (MR_LOGIC_ERROR). */
 mr_status mr_scene_create_with(const mr_scene_desc* desc, const mr_bvh_desc* bvh,
                                const mr_build_settings* build, mr_scene** scene);
 
 /* Releases every device and host resource of the scene. */
 mr_status mr_scene_destroy(mr_scene* scene);
+
+/* Refit of a two-level scene, no reference counterpart (the reference rebuilds its flattened
+ * tree for every new snapshot, src/render/bvh.cpp:31-99). Replaces the transforms
+ * (object_to_world, normal_to_world) of instances [first, first + count) with those of
+ * `instances` (their mesh and material must be unchanged) and rebuilds the instance-level tree;
+ * every mesh tree is reused. The scene then renders exactly as a scene created from the updated
+ * description. Emissive instances cannot move (their triangles are the scene's area lights):
+ * MR_INVALID_ARGUMENT, as for a flattened scene. Not thread-safe against rendering the same
+ * scene. */
+mr_status mr_scene_update_instances(mr_scene* scene, uint32_t first, uint32_t count,
+                                    const mr_instance* instances);
+
+/* Refit of a two-level scene, no reference counterpart: replaces the object-space positions of
+ * mesh `mesh` (same position count, same triangles) and refits its tree bottom-up (the topology
+ * is kept, the boxes are recomputed), then rebuilds the instance-level tree. Meshes used by an
+ * emissive instance cannot change (MR_INVALID_ARGUMENT). */
+mr_status mr_scene_update_mesh(mr_scene* scene, uint32_t mesh, const float* positions,
+                               uint32_t position_count);
+
+/* Device bytes held by the scene (geometry, trees, light and material tables). No reference
+ * counterpart. */
+mr_status mr_scene_device_bytes(const mr_scene* scene, uint64_t* bytes);
 
 /* SceneBvh::statistics (include/minirender/render/bvh.hpp:52). */
 mr_status mr_scene_bvh_statistics(const mr_scene* scene, mr_bvh_statistics* statistics);

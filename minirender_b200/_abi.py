@@ -99,7 +99,7 @@ class BvhDesc(C.Structure):
 
 class BuildSettings(C.Structure):
     _fields_ = [("split_references", C.c_uint32), ("split_factor", C.c_float),
-                ("max_references", C.c_uint64)]
+                ("max_references", C.c_uint64), ("two_level", C.c_uint32)]
 
 
 class IntegratorSettings(C.Structure):
@@ -215,6 +215,9 @@ SIGNATURES = {
     "mr_scene_create": (C.c_int, [P(SceneDesc), P(BvhDesc), P(VP)]),
     "mr_scene_create_with": (C.c_int, [P(SceneDesc), P(BvhDesc), P(BuildSettings), P(VP)]),
     "mr_scene_destroy": (C.c_int, [VP]),
+    "mr_scene_update_instances": (C.c_int, [VP, C.c_uint32, C.c_uint32, P(Instance)]),
+    "mr_scene_update_mesh": (C.c_int, [VP, C.c_uint32, P(C.c_float), C.c_uint32]),
+    "mr_scene_device_bytes": (C.c_int, [VP, P(C.c_uint64)]),
     "mr_scene_bvh_statistics": (C.c_int, [VP, P(BvhStatistics)]),
     "mr_scene_sah_cost": (C.c_int, [VP, P(C.c_double)]),
     "mr_scene_export_bvh": (C.c_int, [VP, P(BvhNode), C.c_uint32, P(C.c_uint32), C.c_uint32,

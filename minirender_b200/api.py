@@ -89,13 +89,14 @@ class Scene:
 
     def __init__(self, snapshot: Snapshot | SceneDocument, bvh: _abi.BvhDesc | None = None,
                  split_references: bool = False, split_factor: float = 0.0,
-                 max_references: int = 0):
+                 max_references: int = 0, two_level: bool = False):
         self.lib = load_library()
         if isinstance(snapshot, SceneDocument):
             snapshot = snapshot.snapshot()
         self.snapshot = snapshot
         handle = C.c_void_p()
-        build = _abi.BuildSettings(int(split_references), split_factor, max_references)
+        build = _abi.BuildSettings(int(split_references), split_factor, max_references,
+                                   int(two_level))
         check(self.lib.mr_scene_create_with(snapshot.desc_pointer(),
                                             C.pointer(bvh) if bvh is not None else None,
                                             C.byref(build), C.byref(handle)), self.lib)
@@ -111,6 +112,30 @@ class Scene:
             self.close()
         except Exception:
             pass
+
+    def device_bytes(self) -> int:
+        """Device memory the scene holds (geometry, trees, light and material tables)."""
+        v = C.c_uint64()
+        check(self.lib.mr_scene_device_bytes(self.handle, C.byref(v)), self.lib)
+        return v.value
+
+    def update_instances(self, first: int, document: SceneDocument):
+        """Two-level scenes: takes the transforms of instances [first, first + k) from
+        `document`'s objects first.. (same meshes and materials) and rebuilds the instance
+        tree (mr_scene_update_instances)."""
+        snap = document.snapshot()
+        desc = snap.desc
+        count = desc.instance_count - first
+        base = C.addressof(desc.instances.contents) + first * C.sizeof(_abi.Instance)
+        check(self.lib.mr_scene_update_instances(self.handle, first, count,
+                                                 C.cast(base, C.POINTER(_abi.Instance))), self.lib)
+
+    def update_mesh(self, mesh: int, positions):
+        """Two-level scenes: new object-space positions (same count) of mesh `mesh`, whose tree is
+        refit (mr_scene_update_mesh)."""
+        p = np.ascontiguousarray(positions, np.float32).reshape(-1, 3)
+        check(self.lib.mr_scene_update_mesh(self.handle, mesh, _ptr(p, C.c_float), p.shape[0]),
+              self.lib)
 
     def statistics(self) -> dict:
         s = _abi.BvhStatistics()

@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "errors.hpp"
+#include "instancing.cuh"
 #include "shading.cuh"
 #include "validation.hpp"
 #include "wavefront.cuh"
@@ -116,16 +117,18 @@ __global__ void query_kernel(DeviceScene s, const mr_ray* rays, size_t count, in
         q.init(make(r.origin[0], r.origin[1], r.origin[2]),
                make(r.direction[0], r.direction[1], r.direction[2]));
         if (any_hit) {
-            const TraceResult t = trace<true>(s, q, r.minimum, r.maximum, tc, err);
+            const TraceResult t = s.two_level ? trace2<true>(s, q, r.minimum, r.maximum, tc, err)
+                                              : trace<true>(s, q, r.minimum, r.maximum, tc, err);
             occluded[i]         = t.slot != kNone ? 1 : 0;
         } else {
-            const TraceResult t = trace<false>(s, q, r.minimum, r.maximum, tc, err);
+            const TraceResult t = s.two_level ? trace2<false>(s, q, r.minimum, r.maximum, tc, err)
+                                              : trace<false>(s, q, r.minimum, r.maximum, tc, err);
             mr_hit            h{};
             h.primitive = kNone;
             if (t.slot != kNone) {
                 const float b0 = __fdiv_rn(t.a, t.det), b1 = __fdiv_rn(t.b, t.det),
                             b2 = __fdiv_rn(t.c, t.det);
-                const SurfaceHit sh = surface_hit(s, q.d, t.slot, b0, b1, b2);
+                const SurfaceHit sh = surface_hit<true>(s, q.d, t.slot, b0, b1, b2);
                 h.distance       = t.t;
                 h.instance_index = sh.instance;
                 h.triangle_index = sh.triangle;
@@ -462,8 +465,8 @@ mr_status mr_scene_create_with(const mr_scene_desc* desc, const mr_bvh_desc* bvh
                                const mr_build_settings* build, mr_scene** scene) {
     return guarded([&] {
         require(desc != nullptr && scene != nullptr, "Scene descriptor or output is null");
-        require(!(bvh && build && build->split_references),
-                "Split references apply to the GPU builder, not to an imported tree");
+        require(!(bvh && build && (build->split_references || build->two_level)),
+                "Split references and two levels apply to the GPU builder, not to an imported tree");
         auto s  = std::make_unique<mr_scene>();
         s->impl = create_scene(*desc, bvh, build);
         *scene  = s.release();
@@ -472,6 +475,29 @@ mr_status mr_scene_create_with(const mr_scene_desc* desc, const mr_bvh_desc* bvh
 
 mr_status mr_scene_destroy(mr_scene* scene) {
     return guarded([&] { delete scene; });
+}
+
+mr_status mr_scene_update_instances(mr_scene* scene, uint32_t first, uint32_t count,
+                                    const mr_instance* instances) {
+    return guarded([&] {
+        require(scene != nullptr && scene->impl != nullptr, "Scene handle is null");
+        update_instances(*scene->impl, first, count, instances);
+    });
+}
+
+mr_status mr_scene_update_mesh(mr_scene* scene, uint32_t mesh, const float* positions,
+                               uint32_t position_count) {
+    return guarded([&] {
+        require(scene != nullptr && scene->impl != nullptr, "Scene handle is null");
+        update_mesh(*scene->impl, mesh, positions, position_count);
+    });
+}
+
+mr_status mr_scene_device_bytes(const mr_scene* scene, uint64_t* bytes) {
+    return guarded([&] {
+        require(bytes != nullptr, "Output is null");
+        *bytes = scene_of(scene).device_bytes;
+    });
 }
 
 mr_status mr_scene_bvh_statistics(const mr_scene* scene, mr_bvh_statistics* statistics) {
@@ -488,6 +514,9 @@ mr_status mr_scene_export_bvh(const mr_scene* scene, mr_bvh_node* nodes, uint32_
         const Scene&   s = scene_of(scene);
         const uint32_t n = static_cast<uint32_t>(s.ref_nodes.count);
         const uint32_t p = s.d.primitive_count;
+        if (s.two) {
+            fail(MR_LOGIC_ERROR, "A two-level scene has no reference-layout export");
+        }
         if (s.references != p) {
             fail(MR_LOGIC_ERROR, "A tree with split references has no reference-layout export");
         }
@@ -516,6 +545,10 @@ mr_status mr_scene_sah_cost(const mr_scene* scene, double* cost) {
     return guarded([&] {
         require(cost != nullptr, "Output is null");
         const Scene& s = scene_of(scene);
+        if (s.two) {
+            fail(MR_LOGIC_ERROR, "A two-level scene has no single tree whose SAH cost compares "
+                                 "with the reference builder's");
+        }
         const size_t n = s.ref_nodes.count;
         *cost          = 0;
         if (n == 0) {

@@ -125,7 +125,7 @@ struct Lane {
     std::shared_ptr<Workspace>                           ws;
     WaveDesc*                                            d_wave = nullptr;
     cudaEvent_t                                          mark   = nullptr;
-    std::map<std::pair<uint32_t, bool>, cudaGraphExec_t> graphs;
+    std::map<std::pair<uint32_t, int>, cudaGraphExec_t> graphs;  // by depth, media | two levels << 1
 };
 
 // Mean of the samples accumulated so far (preview of a running job): pixels in rows < row have
@@ -620,8 +620,8 @@ class Server {
         return true;
     }
 
-    cudaGraphExec_t graph_for(Lane& lane, uint32_t depth, bool media) {
-        const auto key = std::make_pair(depth, media);
+    cudaGraphExec_t graph_for(Lane& lane, uint32_t depth, bool media, bool two) {
+        const auto key = std::make_pair(depth, (media ? 1 : 0) | (two ? 2 : 0));
         auto it = lane.graphs.find(key);
         if (it != lane.graphs.end()) {
             return it->second;
@@ -629,7 +629,7 @@ class Server {
         cudaGraph_t graph = nullptr;
         MR_CUDA(cudaStreamBeginCapture(lane.stream, cudaStreamCaptureModeThreadLocal));
         try {
-            Engine::enqueue_batch_paths(lane.d_wave, depth, media, shape_, *lane.ws, lane.stream);
+            Engine::enqueue_batch_paths(lane.d_wave, depth, media, two, shape_, *lane.ws, lane.stream);
         } catch (...) {
             cudaStreamEndCapture(lane.stream, &graph);
             if (graph) {
@@ -669,7 +669,7 @@ class Server {
         rec.stage            = stage;
         uint64_t space       = settings_.batch.wave_paths;
         uint32_t count = 0, pixels = 0, depth = 0;
-        bool     media = false;
+        bool     media = false, two = false;
         for (Job* j : order) {
             if (rec.pieces.size() == kMaxSegments || space < 32) {
                 break;
@@ -697,6 +697,7 @@ class Server {
             space -= paths;
             depth = std::max(depth, j->p.maximum_depth);
             media = media || j->scene->d.medium_count > 0;
+            two   = two || j->scene->d.two_level != 0;
             j->issued = after;
             j->issued_samples += paths;
             rec.pieces.push_back({j, after, paths, after.sample >= j->spp});
@@ -729,10 +730,10 @@ class Server {
         MR_CUDA(cudaMemcpyAsync(lane.d_wave, &h, bytes, cudaMemcpyHostToDevice, lane.stream));
         MR_CUDA(cudaEventRecord(rec.start, lane.stream));
         if (settings_.batch.use_graphs) {
-            MR_CUDA(cudaGraphLaunch(graph_for(lane, depth, media), lane.stream));
+            MR_CUDA(cudaGraphLaunch(graph_for(lane, depth, media, two), lane.stream));
             ++stats_.graph_launches;
         } else {
-            Engine::enqueue_batch_paths(lane.d_wave, depth, media, shape_, *lane.ws, lane.stream);
+            Engine::enqueue_batch_paths(lane.d_wave, depth, media, two, shape_, *lane.ws, lane.stream);
         }
         // Resolves run in wave order across lanes: per pixel, samples accumulate in order.
         MR_CUDA(cudaStreamWaitEvent(lane.stream, resolve_chain_, 0));

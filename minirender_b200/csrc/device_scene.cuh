@@ -23,6 +23,35 @@
 
 namespace mr {
 
+// glm::vec3(object_to_world * glm::vec4(p, 1)) in float with GLM's evaluation order
+// (m0*x + m1*y) + (m2*z + m3*w) and no fused operations (src/render/bvh.cpp:68-69). Host and
+// device produce identical world vertices; a two-level scene evaluates it during traversal and
+// gets the flattened scene's vertices bit for bit.
+MR_HD f3 transform_point(const float* m, float x, float y, float z) {
+#ifdef __CUDA_ARCH__
+    const auto row = [&](int r) {
+        return __fadd_rn(__fadd_rn(__fmul_rn(m[r], x), __fmul_rn(m[4 + r], y)),
+                         __fadd_rn(__fmul_rn(m[8 + r], z), __fmul_rn(m[12 + r], 1.0f)));
+    };
+#else
+    const auto row = [&](int r) {
+        volatile float a = m[r] * x, b = m[4 + r] * y, c = m[8 + r] * z, d = m[12 + r] * 1.0f;
+        volatile float ab = a + b, cd = c + d;
+        return static_cast<float>(ab + cd);
+    };
+#endif
+    return {row(0), row(1), row(2)};
+}
+
+// normalize(normal_to_world * n) of a mesh corner normal (src/render/bvh.cpp:319-320), with the
+// multiply-adds fused explicitly so every kernel that evaluates it gets the same bits.
+__device__ __forceinline__ f3 world_normal(const float* m, const float* n) {
+    const f3 w = {fmaf(m[6], n[2], fmaf(m[3], n[1], m[0] * n[0])),
+                  fmaf(m[7], n[2], fmaf(m[4], n[1], m[1] * n[0])),
+                  fmaf(m[8], n[2], fmaf(m[5], n[1], m[2] * n[0]))};
+    return normalize(w);
+}
+
 enum TriFlags : unsigned {
     kTriSingleSided = 1u,
     kTriMirrored    = 2u,
@@ -60,6 +89,40 @@ struct DeviceMedium {
 
 constexpr int kMaxMedia = 32;  // maximum_medium_regions (include/minirender/scene/medium.hpp:43)
 
+// One instance of a two-level scene: where its mesh tree (BLAS) starts, how it maps to world
+// space, and the bounds the traversal needs. `to_world` is the column-major object_to_world of
+// the snapshot (the flattening's matrix); `to_object` its FP32 inverse affine, row-major 3x4.
+struct DeviceInstance2 {
+    float    to_world[16];
+    float    to_object[12];
+    float    normal_to_world[9];
+    float    lo[3], hi[3];    // world box of the instance's triangles, grown to cover rounding
+    float    margin_static;   // object-space growth of mesh boxes for the world vertices' rounding
+    float    a_norm, b_norm;  // infinity norms of to_object's linear part and translation
+    int      blas_root;       // >= 0 wide node of blas_nodes, < 0 leaf ~slot of blas_tris
+    uint32_t first_prim;      // flat primitive id of the instance's first triangle
+    uint32_t position_offset; // into mesh_positions (vertices)
+    uint32_t corner_offset;   // into mesh_corners (3 per triangle)
+    uint32_t material;
+    uint32_t flags;           // kTriSingleSided | kTriMirrored | kTriEmissive | kind << 8
+};
+
+// The instance of a two-level scene holding flat primitive `prim` (the last instance whose first
+// primitive is at most `prim`).
+__device__ __forceinline__ uint32_t find_instance2(const DeviceInstance2* instances, uint32_t count,
+                                                   uint32_t prim) {
+    uint32_t lo = 0, hi = count;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(&instances[mid].first_prim) <= prim) {
+            lo = mid;
+        } else {
+            hi = mid;
+        }
+    }
+    return lo;
+}
+
 struct CameraBasis {
     f3    position;
     f3    forward, right, up;
@@ -89,6 +152,19 @@ struct DeviceScene {
     int                   medium_count;
     int                   media_scatter;    // any region scatters
     CameraBasis           camera;
+    // Two-level scenes (two_level != 0): `nodes` and `root` are the instance-level tree, whose
+    // leaves list instance ids in tlas_items (bit 31 marks a leaf's last item); every mesh has
+    // its own object-space tree in blas_nodes over object-space triangle slots in blas_tris
+    // ([0] = v0.xyz + triangle index within the mesh, [1] = v1.xyz + kTriLeafEnd, [2] = v2.xyz).
+    // The meshes' positions and corners stay resident for shading.
+    int                    two_level;
+    uint32_t               instance_count;
+    const DeviceInstance2* instances;
+    const uint32_t*        tlas_items;
+    const float4*          blas_nodes;
+    const float4*          blas_tris;
+    const float*           mesh_positions;
+    const mr_mesh_corner*  mesh_corners;
 };
 
 }  // namespace mr

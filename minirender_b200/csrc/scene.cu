@@ -12,30 +12,13 @@
 #include <numeric>
 
 #include "errors.hpp"
+#include "instancing.cuh"
 #include "scan.cuh"
 #include "scene.cuh"
 
 namespace mr {
 
 namespace {
-
-// glm::vec3(object_to_world * glm::vec4(p, 1)) in float with GLM's evaluation order
-// (m0*x + m1*y) + (m2*z + m3*w) and no fused operations (src/render/bvh.cpp:68-69).
-MR_HD f3 transform_point(const float* m, float x, float y, float z) {
-#ifdef __CUDA_ARCH__
-    const auto row = [&](int r) {
-        return __fadd_rn(__fadd_rn(__fmul_rn(m[r], x), __fmul_rn(m[4 + r], y)),
-                         __fadd_rn(__fmul_rn(m[8 + r], z), __fmul_rn(m[12 + r], 1.0f)));
-    };
-#else
-    const auto row = [&](int r) {
-        volatile float a = m[r] * x, b = m[4 + r] * y, c = m[8 + r] * z, d = m[12 + r] * 1.0f;
-        volatile float ab = a + b, cd = c + d;
-        return static_cast<float>(ab + cd);
-    };
-#endif
-    return {row(0), row(1), row(2)};
-}
 
 struct DeviceInstance {
     float    object_to_world[16];
@@ -80,11 +63,7 @@ __global__ void flatten_kernel(const float* positions, const mr_mesh_corner* cor
         const mr_mesh_corner& corner = corners[inst.corner_offset + 3 * tri + c];
         const float*          q      = positions + 3 * (static_cast<size_t>(inst.position_offset) + corner.position);
         v[c] = transform_point(inst.object_to_world, q[0], q[1], q[2]);
-        const float* m = inst.normal_to_world;
-        const f3 w = {(m[0] * corner.normal[0] + m[3] * corner.normal[1]) + m[6] * corner.normal[2],
-                      (m[1] * corner.normal[0] + m[4] * corner.normal[1]) + m[7] * corner.normal[2],
-                      (m[2] * corner.normal[0] + m[5] * corner.normal[1]) + m[8] * corner.normal[2]};
-        n[c] = normalize(w);
+        n[c] = world_normal(inst.normal_to_world, corner.normal);
     }
     if (!finite3(v[0]) || !finite3(v[1]) || !finite3(v[2])) {
         atomicOr(error, 1u);
@@ -337,12 +316,6 @@ void validate_media(const mr_medium_region* media, uint32_t count) {
     }
 }
 
-float determinant3(const float* m) {
-    const auto e = [m](int c, int r) { return m[4 * c + r]; };
-    return e(0, 0) * (e(1, 1) * e(2, 2) - e(2, 1) * e(1, 2)) -
-           e(1, 0) * (e(0, 1) * e(2, 2) - e(2, 1) * e(0, 2)) +
-           e(2, 0) * (e(0, 1) * e(1, 2) - e(1, 1) * e(0, 2));
-}
 
 void validate_imported(const mr_bvh_desc& b, uint32_t prims) {
     require(b.primitive_count == prims, "Imported BVH primitive count differs from the scene");
@@ -373,6 +346,193 @@ void validate_imported(const mr_bvh_desc& b, uint32_t prims) {
 }
 
 }  // namespace
+
+float determinant3(const float* m) {
+    const auto e = [m](int c, int r) { return m[4 * c + r]; };
+    return e(0, 0) * (e(1, 1) * e(2, 2) - e(2, 1) * e(1, 2)) -
+           e(1, 0) * (e(0, 1) * e(2, 2) - e(2, 1) * e(0, 2)) +
+           e(2, 0) * (e(0, 1) * e(1, 2) - e(1, 1) * e(0, 2));
+}
+
+WideTree collapse_tree(const mr_bvh_node* ref_nodes, uint32_t node_count, cudaStream_t stream) {
+    WideTree out;
+    if (node_count == 0) {
+        return out;
+    }
+    mr_bvh_node root{};
+    MR_CUDA(cudaMemcpyAsync(&root, ref_nodes, sizeof(root), cudaMemcpyDeviceToHost, stream));
+    DeviceBuffer<uint32_t> total;
+    total.allocate(1);
+    MR_CUDA(cudaMemsetAsync(total.ptr, 0, sizeof(uint32_t), stream));
+    interior_count_kernel<<<(node_count + 255) / 256, 256, 0, stream>>>(ref_nodes, node_count, total.ptr);
+    uint32_t interior = 0;
+    MR_CUDA(cudaMemcpyAsync(&interior, total.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+    MR_CUDA(cudaStreamSynchronize(stream));
+    for (int a = 0; a < 3; ++a) {
+        out.lo[a] = root.minimum[a];
+        out.hi[a] = root.maximum[a];
+    }
+    out.root_count = root.count;
+    out.nodes.allocate(std::max<uint32_t>(1, interior) * 8ull);
+    out.children.allocate(std::max<uint32_t>(1, interior));
+    if (interior == 0) {
+        return out;
+    }
+    DeviceBuffer<uint32_t> roots[2], counts, offsets, scratch;
+    roots[0].allocate(interior);
+    roots[1].allocate(interior);
+    counts.allocate(interior);
+    offsets.allocate(interior);
+    scratch.allocate(scan_scratch_size(interior));
+    MR_CUDA(cudaMemsetAsync(roots[0].ptr, 0, sizeof(uint32_t), stream));  // the root
+    uint32_t level = 1, base = 0, cur = 0;
+    while (level > 0) {
+        int4* children = out.children.ptr + base;
+        collapse_count_kernel<<<(level + 127) / 128, 128, 0, stream>>>(ref_nodes, roots[cur].ptr, level,
+                                                                       children, counts.ptr);
+        exclusive_scan(counts.ptr, offsets.ptr, level, scratch.ptr, total.ptr, stream);
+        collapse_write_kernel<<<(level + 127) / 128, 128, 0, stream>>>(
+            ref_nodes, children, level, offsets.ptr, base, base + level, out.nodes.ptr, roots[cur ^ 1].ptr);
+        uint32_t next = 0;
+        MR_CUDA(cudaMemcpyAsync(&next, total.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+        MR_CUDA(cudaStreamSynchronize(stream));
+        base += level;
+        level = next;
+        cur ^= 1;
+    }
+    out.count = base;
+    return out;
+}
+
+void mark_leaf_ends(const mr_bvh_node* nodes, uint32_t node_count, float4* tris, cudaStream_t stream) {
+    if (node_count) {
+        mark_leaf_end_kernel<<<(node_count + 255) / 256, 256, 0, stream>>>(nodes, node_count, tris);
+        MR_CUDA(cudaGetLastError());
+    }
+}
+
+// DiscreteDistribution (src/core/sampling.cpp:109-127) in FP32 over the light weights, the
+// directional and environment weights scaled by the projected area of the world bounds.
+void upload_light_table(Scene& scene, const float* lo, const float* hi, cudaStream_t stream) {
+    const LightTable& t = scene.light_table;
+    float projected_area = kPi;
+    if (scene.d.primitive_count) {
+        const f3 extent = {hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2]};
+        projected_area  = kPi * std::max(dot(extent, extent) * 0.25f, 1e-12f);
+    }
+    std::vector<float> weights(t.weights.size());
+    for (size_t i = 0; i < weights.size(); ++i) {
+        weights[i] = t.scales[i] ? projected_area * t.weights[i] : t.weights[i];
+    }
+    std::vector<float> cdf(weights.size() + 1, 0.0f);
+    float maximum = 0;
+    for (float w : weights) {
+        require(std::isfinite(w) && w >= 0, "Distribution weights must be finite and nonnegative");
+        maximum = std::max(maximum, w);
+    }
+    for (size_t i = 0; i < weights.size(); ++i) {
+        cdf[i + 1] = cdf[i] + (maximum > 0 ? weights[i] / maximum : 1.0f);
+    }
+    if (!weights.empty()) {
+        const float integral_cdf = cdf.back();
+        for (auto& v : cdf) {
+            v /= integral_cdf;
+        }
+    }
+    scene.d.light_count = static_cast<uint32_t>(t.lights.size());
+    if (!scene.lights.ptr) {
+        scene.lights.allocate(std::max<size_t>(1, t.lights.size()));
+        if (!t.lights.empty()) {
+            MR_CUDA(cudaMemcpyAsync(scene.lights.ptr, t.lights.data(), t.lights.size() * sizeof(DeviceLight),
+                                    cudaMemcpyHostToDevice, stream));
+        }
+    }
+    if (!scene.light_cdf.ptr) {
+        scene.light_cdf.allocate(cdf.size());
+    }
+    MR_CUDA(cudaMemcpyAsync(scene.light_cdf.ptr, cdf.data(), cdf.size() * sizeof(float), cudaMemcpyHostToDevice,
+                            stream));
+    // The copy reads host memory that goes away with this function.
+    MR_CUDA(cudaStreamSynchronize(stream));
+    scene.d.lights    = scene.lights.ptr;
+    scene.d.light_cdf = scene.light_cdf.ptr;
+}
+
+// The host light table and the primitive -> emitter map: area lights in instance and triangle
+// order, then directional lights, then the constant environment.
+void build_light_table(Scene& scene, const mr_scene_desc& desc, const std::vector<uint32_t>& first_prim,
+                       cudaStream_t stream) {
+    LightTable&           t     = scene.light_table;
+    const uint32_t        prims = scene.d.primitive_count;
+    std::vector<uint32_t> emitter_of_prim(std::max<uint32_t>(1, prims), kNone);
+    t = LightTable{};
+    for (uint32_t i = 0; i < desc.instance_count; ++i) {
+        const mr_instance& in  = desc.instances[i];
+        const mr_material& mat = desc.materials[in.material];
+        const f3 radiance = {mat.emission[0], mat.emission[1], mat.emission[2]};
+        if (luminance(radiance) == 0) {
+            continue;
+        }
+        const mr_mesh& mesh        = desc.meshes[in.mesh];
+        const float    orientation = determinant3(in.object_to_world) < 0 ? -1.0f : 1.0f;
+        for (uint32_t tri = 0; tri < mesh.triangle_count; ++tri) {
+            f3 v[3];
+            for (int c = 0; c < 3; ++c) {
+                const float* p = mesh.positions + 3 * mesh.corners[3 * tri + c].position;
+                v[c]           = transform_point(in.object_to_world, p[0], p[1], p[2]);
+            }
+            const f3    cr   = cross(v[1] - v[0], v[2] - v[0]);
+            const float area = length(cr) * 0.5f;
+            if (area == 0) {
+                continue;
+            }
+            DeviceLight l{};
+            l.v0 = v[0];
+            l.v1 = v[1];
+            l.v2 = v[2];
+            l.normal       = cr * orientation / (2.0f * area);
+            l.radiance     = radiance;
+            l.area         = area;
+            l.kind         = kLightArea;
+            l.double_sided = mat.double_sided;
+            emitter_of_prim[first_prim[i] + tri] = static_cast<uint32_t>(t.lights.size());
+            t.lights.push_back(l);
+            t.weights.push_back((mat.double_sided ? 2.0f : 1.0f) * kPi * area * luminance(radiance));
+            t.scales.push_back(0);
+        }
+    }
+    for (uint32_t i = 0; i < desc.directional_light_count; ++i) {
+        const auto& dl       = desc.directional_lights[i];
+        const f3    radiance = f3{dl.color[0], dl.color[1], dl.color[2]} * dl.intensity;
+        if (luminance(radiance) > 0) {
+            DeviceLight l{};
+            l.normal   = -normalize(f3{dl.direction[0], dl.direction[1], dl.direction[2]});
+            l.radiance = radiance;
+            l.kind     = kLightDirectional;
+            t.lights.push_back(l);
+            t.weights.push_back(luminance(radiance));
+            t.scales.push_back(1);
+        }
+    }
+    const f3 environment        = {desc.environment[0], desc.environment[1], desc.environment[2]};
+    scene.d.environment         = environment;
+    scene.d.environment_choice  = -1;
+    const float integral        = 4.0f * kPi * luminance(environment);
+    if (integral > 0) {
+        DeviceLight l{};
+        l.radiance                 = environment;
+        l.kind                     = kLightEnvironment;
+        scene.d.environment_choice = static_cast<int>(t.lights.size());
+        t.lights.push_back(l);
+        t.weights.push_back(integral);
+        t.scales.push_back(1);
+    }
+    scene.prim_emitter.allocate(emitter_of_prim.size());
+    MR_CUDA(cudaMemcpyAsync(scene.prim_emitter.ptr, emitter_of_prim.data(),
+                            emitter_of_prim.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+    MR_CUDA(cudaStreamSynchronize(stream));  // the source vector goes away with this function
+    scene.d.prim_emitter = scene.prim_emitter.ptr;
+}
 
 cudaMemPool_t library_pool() {
     static std::mutex                  mutex;
@@ -505,158 +665,170 @@ std::unique_ptr<Scene> create_scene(const mr_scene_desc& desc, const mr_bvh_desc
                                 instances.size() * sizeof(DeviceInstance), cudaMemcpyHostToDevice, stream));
     }
 
-    // ---- flatten ----
-    DeviceBuffer<float4>   world, lo, hi, centroid;
-    DeviceBuffer<uint32_t> error;
-    world.allocate(3ull * prims);
-    scene->shading.allocate(3ull * prims);
-    lo.allocate(prims);
-    hi.allocate(prims);
-    centroid.allocate(prims);
-    error.allocate(1);
-    MR_CUDA(cudaMemsetAsync(error.ptr, 0, sizeof(uint32_t), stream));
-    if (prims) {
-        flatten_kernel<<<(prims + 255) / 256, 256, 0, stream>>>(
-            positions.ptr, corners.ptr, reinterpret_cast<const DeviceInstance*>(instance_buffer.ptr),
-            desc.instance_count, prims, world.ptr, scene->shading.ptr, lo.ptr, hi.ptr, centroid.ptr,
-            error.ptr);
-        MR_CUDA(cudaGetLastError());
+    std::vector<uint32_t> first_prim(desc.instance_count);
+    for (uint32_t i = 0; i < desc.instance_count; ++i) {
+        first_prim[i] = instances[i].first_prim;
     }
-    uint32_t flatten_error = 0;
-    MR_CUDA(cudaMemcpyAsync(&flatten_error, error.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
-    MR_CUDA(cudaStreamSynchronize(stream));
-    require(!(flatten_error & 1u), "Transformed triangle position is not finite");
-    require(!(flatten_error & 2u), "Transform collapses a triangle at float precision");
-    positions.release();
-    corners.release();
+    if (build && build->two_level) {
+        // ---- two levels: a tree per mesh in object space under a tree over the instances ----
+        require(!bvh, "A two-level scene builds its own trees; an imported tree is a flattened one");
+        require(!build->split_references, "Split references apply to the flattened tree only");
+        scene->two = {new TwoLevel, [](TwoLevel* t) { delete t; }};
+        TwoLevel& t       = *scene->two;
+        t.positions       = std::move(positions);
+        t.corners         = std::move(corners);
+        t.position_offset = mesh_position_offset;
+        t.corner_offset   = mesh_corner_offset;
+        t.used.assign(desc.mesh_count, 0);
+        t.emissive_mesh.assign(desc.mesh_count, 0);
+        t.host_instances.resize(desc.instance_count);
+        t.instance_mesh.resize(desc.instance_count);
+        t.instance_material.resize(desc.instance_count);
+        for (uint32_t i = 0; i < desc.instance_count; ++i) {
+            const mr_instance& in = desc.instances[i];
+            DeviceInstance2&   d  = t.host_instances[i];
+            d                     = DeviceInstance2{};
+            fill_instance_transform(in, d);
+            d.first_prim          = instances[i].first_prim;
+            d.position_offset     = instances[i].position_offset;
+            d.corner_offset       = instances[i].corner_offset;
+            d.material            = in.material;
+            d.flags               = instances[i].flags;
+            t.instance_mesh[i]     = in.mesh;
+            t.instance_material[i] = in.material;
+            if (instances[i].triangle_count) {
+                t.used[in.mesh] = 1;
+            }
+            if (instances[i].flags & kTriEmissive) {
+                t.emissive_mesh[in.mesh] = 1;
+            }
+        }
+        build_mesh_trees(*scene, desc, stream);
+        build_instance_tree(*scene, stream);
+        scene->references           = prims;
+        scene->statistics.triangles = prims;
+    } else {
+        // ---- flatten ----
+        DeviceBuffer<float4>   world, lo, hi, centroid;
+        DeviceBuffer<uint32_t> error;
+        world.allocate(3ull * prims);
+        scene->shading.allocate(3ull * prims);
+        lo.allocate(prims);
+        hi.allocate(prims);
+        centroid.allocate(prims);
+        error.allocate(1);
+        MR_CUDA(cudaMemsetAsync(error.ptr, 0, sizeof(uint32_t), stream));
+        if (prims) {
+            flatten_kernel<<<(prims + 255) / 256, 256, 0, stream>>>(
+                positions.ptr, corners.ptr, reinterpret_cast<const DeviceInstance*>(instance_buffer.ptr),
+                desc.instance_count, prims, world.ptr, scene->shading.ptr, lo.ptr, hi.ptr, centroid.ptr,
+                error.ptr);
+            MR_CUDA(cudaGetLastError());
+        }
+        uint32_t flatten_error = 0;
+        MR_CUDA(cudaMemcpyAsync(&flatten_error, error.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+        MR_CUDA(cudaStreamSynchronize(stream));
+        require(!(flatten_error & 1u), "Transformed triangle position is not finite");
+        require(!(flatten_error & 2u), "Transform collapses a triangle at float precision");
+        positions.release();
+        corners.release();
 
-    // ---- BVH (reference layout on the device) ----
-    DeviceBuffer<mr_bvh_node> ref_nodes;
-    DeviceBuffer<uint32_t>    ref_order;
-    uint32_t                  node_count = 0;
-    if (prims) {
-        if (bvh) {
-            node_count = bvh->node_count;
-            ref_nodes.allocate(node_count);
-            ref_order.allocate(prims);
-            MR_CUDA(cudaMemcpyAsync(ref_nodes.ptr, bvh->nodes, node_count * sizeof(mr_bvh_node),
-                                    cudaMemcpyHostToDevice, stream));
-            MR_CUDA(cudaMemcpyAsync(ref_order.ptr, bvh->order, prims * sizeof(uint32_t),
-                                    cudaMemcpyHostToDevice, stream));
-            // Statistics of the imported tree (host walk).
-            std::vector<std::pair<uint32_t, uint32_t>> stack{{0u, 0u}};
-            uint64_t leaves = 0, depth = 0;
-            while (!stack.empty()) {
-                const auto [i, d] = stack.back();
-                stack.pop_back();
-                depth = std::max<uint64_t>(depth, d);
-                const auto& n = bvh->nodes[i];
-                if (n.count) {
-                    ++leaves;
-                } else {
-                    require(d < 64, "Imported BVH is deeper than 64 levels");
-                    stack.push_back({n.first, d + 1});
-                    stack.push_back({n.right, d + 1});
+        // ---- BVH (reference layout on the device) ----
+        DeviceBuffer<mr_bvh_node> ref_nodes;
+        DeviceBuffer<uint32_t>    ref_order;
+        uint32_t                  node_count = 0;
+        if (prims) {
+            if (bvh) {
+                node_count = bvh->node_count;
+                ref_nodes.allocate(node_count);
+                ref_order.allocate(prims);
+                MR_CUDA(cudaMemcpyAsync(ref_nodes.ptr, bvh->nodes, node_count * sizeof(mr_bvh_node),
+                                        cudaMemcpyHostToDevice, stream));
+                MR_CUDA(cudaMemcpyAsync(ref_order.ptr, bvh->order, prims * sizeof(uint32_t),
+                                        cudaMemcpyHostToDevice, stream));
+                // Statistics of the imported tree (host walk).
+                std::vector<std::pair<uint32_t, uint32_t>> stack{{0u, 0u}};
+                uint64_t leaves = 0, depth = 0;
+                while (!stack.empty()) {
+                    const auto [i, d] = stack.back();
+                    stack.pop_back();
+                    depth = std::max<uint64_t>(depth, d);
+                    const auto& n = bvh->nodes[i];
+                    if (n.count) {
+                        ++leaves;
+                    } else {
+                        require(d < 64, "Imported BVH is deeper than 64 levels");
+                        stack.push_back({n.first, d + 1});
+                        stack.push_back({n.right, d + 1});
+                    }
                 }
+                scene->statistics.leaves        = leaves;
+                scene->statistics.maximum_depth = depth;
+            } else {
+                SplitReferences split;
+                if (build && build->split_references) {
+                    const float    factor = build->split_factor > 0 ? build->split_factor : 16.0f;
+                    const uint64_t cap    = build->max_references
+                                                ? build->max_references
+                                                : std::max<uint64_t>(2ull * prims, prims + 65536ull);
+                    require(std::isfinite(factor) && cap >= prims && cap <= 0xFFFFFFFFull,
+                            "Split settings need a finite factor and a reference cap of at least the "
+                            "triangle count");
+                    split = split_references(world.ptr, lo.ptr, hi.ptr, prims, factor, cap, stream);
+                }
+                const uint32_t refs  = split.count ? split.count : prims;
+                BuildResult    built = split.count
+                                           ? build_bvh_device(split.lo.ptr, split.hi.ptr, split.centroid.ptr, refs, stream)
+                                           : build_bvh_device(lo.ptr, hi.ptr, centroid.ptr, prims, stream);
+                if (split.count) {
+                    map_order_to_primitives(built.order.ptr, split.prim.ptr, refs, stream);
+                }
+                ref_nodes             = std::move(built.nodes);
+                ref_order             = std::move(built.order);
+                node_count            = built.node_count;
+                scene->statistics.leaves        = built.leaves;
+                scene->statistics.maximum_depth = built.maximum_depth;
+                scene->build_seconds  = built.seconds;
+                scene->references     = refs;
             }
-            scene->statistics.leaves        = leaves;
-            scene->statistics.maximum_depth = depth;
-        } else {
-            SplitReferences split;
-            if (build && build->split_references) {
-                const float    factor = build->split_factor > 0 ? build->split_factor : 16.0f;
-                const uint64_t cap    = build->max_references
-                                            ? build->max_references
-                                            : std::max<uint64_t>(2ull * prims, prims + 65536ull);
-                require(std::isfinite(factor) && cap >= prims && cap <= 0xFFFFFFFFull,
-                        "Split settings need a finite factor and a reference cap of at least the "
-                        "triangle count");
-                split = split_references(world.ptr, lo.ptr, hi.ptr, prims, factor, cap, stream);
-            }
-            const uint32_t refs  = split.count ? split.count : prims;
-            BuildResult    built = split.count
-                                       ? build_bvh_device(split.lo.ptr, split.hi.ptr, split.centroid.ptr, refs, stream)
-                                       : build_bvh_device(lo.ptr, hi.ptr, centroid.ptr, prims, stream);
-            if (split.count) {
-                map_order_to_primitives(built.order.ptr, split.prim.ptr, refs, stream);
-            }
-            ref_nodes             = std::move(built.nodes);
-            ref_order             = std::move(built.order);
-            node_count            = built.node_count;
-            scene->statistics.leaves        = built.leaves;
-            scene->statistics.maximum_depth = built.maximum_depth;
-            scene->build_seconds  = built.seconds;
-            scene->references     = refs;
         }
-    }
-    if (scene->references == 0) {
-        scene->references = prims;
-    }
-    const uint32_t slots = scene->references;
-    scene->statistics.triangles = prims;
-    scene->statistics.nodes     = node_count;
-    lo.release();
-    hi.release();
-    centroid.release();
+        if (scene->references == 0) {
+            scene->references = prims;
+        }
+        const uint32_t slots = scene->references;
+        scene->statistics.triangles = prims;
+        scene->statistics.nodes     = node_count;
+        lo.release();
+        hi.release();
+        centroid.release();
 
-    // ---- traversal layout: 4-wide nodes collapsed from the binary tree ----
-    uint32_t wide_count = 0;
-    if (prims) {
-        DeviceBuffer<uint32_t> total;
-        total.allocate(1);
-        MR_CUDA(cudaMemsetAsync(total.ptr, 0, sizeof(uint32_t), stream));
-        interior_count_kernel<<<(node_count + 255) / 256, 256, 0, stream>>>(ref_nodes.ptr, node_count, total.ptr);
-        uint32_t interior = 0;
-        MR_CUDA(cudaMemcpyAsync(&interior, total.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
-        MR_CUDA(cudaStreamSynchronize(stream));
-        scene->nodes.allocate(std::max<uint32_t>(1, interior) * 8ull);
-        if (interior) {
-            DeviceBuffer<uint32_t> roots[2], counts, offsets, scratch;
-            DeviceBuffer<int4>     children;
-            roots[0].allocate(interior);
-            roots[1].allocate(interior);
-            counts.allocate(interior);
-            offsets.allocate(interior);
-            children.allocate(interior);
-            scratch.allocate(scan_scratch_size(interior));
-            MR_CUDA(cudaMemsetAsync(roots[0].ptr, 0, sizeof(uint32_t), stream));  // the root
-            uint32_t level = 1, base = 0, cur = 0;
-            while (level > 0) {
-                collapse_count_kernel<<<(level + 127) / 128, 128, 0, stream>>>(ref_nodes.ptr, roots[cur].ptr,
-                                                                               level, children.ptr, counts.ptr);
-                exclusive_scan(counts.ptr, offsets.ptr, level, scratch.ptr, total.ptr, stream);
-                collapse_write_kernel<<<(level + 127) / 128, 128, 0, stream>>>(
-                    ref_nodes.ptr, children.ptr, level, offsets.ptr, base, base + level, scene->nodes.ptr,
-                    roots[cur ^ 1].ptr);
-                uint32_t next = 0;
-                MR_CUDA(cudaMemcpyAsync(&next, total.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
-                MR_CUDA(cudaStreamSynchronize(stream));
-                base += level;
-                level = next;
-                cur ^= 1;
+        // ---- traversal layout: 4-wide nodes collapsed from the binary tree ----
+        uint32_t wide_count = 0;
+        if (prims) {
+            WideTree wide = collapse_tree(ref_nodes.ptr, node_count, stream);
+            scene->nodes  = std::move(wide.nodes);
+            wide_count    = wide.count;
+            scene->tris.allocate(3ull * slots);
+            gather_triangles_kernel<<<(slots + 255) / 256, 256, 0, stream>>>(world.ptr, ref_order.ptr, slots,
+                                                                             scene->tris.ptr);
+            mark_leaf_end_kernel<<<(node_count + 255) / 256, 256, 0, stream>>>(ref_nodes.ptr, node_count,
+                                                                               scene->tris.ptr);
+            MR_CUDA(cudaGetLastError());
+            mr_bvh_node root{};
+            MR_CUDA(cudaMemcpyAsync(&root, ref_nodes.ptr, sizeof(root), cudaMemcpyDeviceToHost, stream));
+            MR_CUDA(cudaStreamSynchronize(stream));
+            scene->d.has_nodes  = 1;
+            scene->d.root       = root.count == 0 ? 0 : ~static_cast<int>(root.first);
+            scene->d.root_count = root.count;
+            for (int a = 0; a < 3; ++a) {
+                scene->d.root_lo[a] = root.minimum[a];
+                scene->d.root_hi[a] = root.maximum[a];
             }
-            wide_count = base;
         }
-        scene->tris.allocate(3ull * slots);
-        gather_triangles_kernel<<<(slots + 255) / 256, 256, 0, stream>>>(world.ptr, ref_order.ptr, slots,
-                                                                         scene->tris.ptr);
-        mark_leaf_end_kernel<<<(node_count + 255) / 256, 256, 0, stream>>>(ref_nodes.ptr, node_count,
-                                                                           scene->tris.ptr);
-        MR_CUDA(cudaGetLastError());
-        mr_bvh_node root{};
-        MR_CUDA(cudaMemcpyAsync(&root, ref_nodes.ptr, sizeof(root), cudaMemcpyDeviceToHost, stream));
-        MR_CUDA(cudaStreamSynchronize(stream));
-        scene->d.has_nodes  = 1;
-        scene->d.root       = root.count == 0 ? 0 : ~static_cast<int>(root.first);
-        scene->d.root_count = root.count;
-        for (int a = 0; a < 3; ++a) {
-            scene->d.root_lo[a] = root.minimum[a];
-            scene->d.root_hi[a] = root.maximum[a];
-        }
+        scene->d.node_count = wide_count;
+        scene->ref_nodes    = std::move(ref_nodes);
+        scene->ref_order    = std::move(ref_order);
     }
-    scene->d.node_count = wide_count;
-    scene->ref_nodes    = std::move(ref_nodes);
-    scene->ref_order    = std::move(ref_order);
 
     // ---- materials ----
     std::vector<DeviceMaterial> materials(std::max<uint32_t>(1, desc.material_count));
@@ -671,101 +843,12 @@ std::unique_ptr<Scene> create_scene(const mr_scene_desc& desc, const mr_bvh_desc
                             cudaMemcpyHostToDevice, stream));
 
     // ---- lights (LightSampler constructor, src/render/light.cpp:197-264) ----
-    std::vector<DeviceLight> lights;
-    std::vector<float>       weights;
-    std::vector<uint32_t>    emitter_of_prim(std::max<uint32_t>(1, prims), kNone);
-    for (uint32_t i = 0; i < desc.instance_count; ++i) {
-        const mr_instance& in  = desc.instances[i];
-        const mr_material& mat = desc.materials[in.material];
-        const f3 radiance = {mat.emission[0], mat.emission[1], mat.emission[2]};
-        if (luminance(radiance) == 0) {
-            continue;
-        }
-        const mr_mesh& mesh        = desc.meshes[in.mesh];
-        const float    orientation = determinant3(in.object_to_world) < 0 ? -1.0f : 1.0f;
-        for (uint32_t t = 0; t < mesh.triangle_count; ++t) {
-            f3 v[3];
-            for (int c = 0; c < 3; ++c) {
-                const float* p = mesh.positions + 3 * mesh.corners[3 * t + c].position;
-                v[c]           = transform_point(in.object_to_world, p[0], p[1], p[2]);
-            }
-            const f3    cr   = cross(v[1] - v[0], v[2] - v[0]);
-            const float area = length(cr) * 0.5f;
-            if (area == 0) {
-                continue;
-            }
-            DeviceLight l{};
-            l.v0 = v[0];
-            l.v1 = v[1];
-            l.v2 = v[2];
-            l.normal       = cr * orientation / (2.0f * area);
-            l.radiance     = radiance;
-            l.area         = area;
-            l.kind         = kLightArea;
-            l.double_sided = mat.double_sided;
-            emitter_of_prim[instances[i].first_prim + t] = static_cast<uint32_t>(lights.size());
-            lights.push_back(l);
-            weights.push_back((mat.double_sided ? 2.0f : 1.0f) * kPi * area * luminance(radiance));
-        }
+    build_light_table(*scene, desc, first_prim, stream);
+    if (scene->two) {
+        upload_light_table(*scene, scene->two->world_lo, scene->two->world_hi, stream);
+    } else {
+        upload_light_table(*scene, scene->d.root_lo, scene->d.root_hi, stream);
     }
-    float projected_area = kPi;
-    if (prims) {
-        const f3 extent = {scene->d.root_hi[0] - scene->d.root_lo[0], scene->d.root_hi[1] - scene->d.root_lo[1],
-                           scene->d.root_hi[2] - scene->d.root_lo[2]};
-        projected_area = kPi * std::max(dot(extent, extent) * 0.25f, 1e-12f);
-    }
-    for (uint32_t i = 0; i < desc.directional_light_count; ++i) {
-        const auto& dl       = desc.directional_lights[i];
-        const f3    radiance = f3{dl.color[0], dl.color[1], dl.color[2]} * dl.intensity;
-        if (luminance(radiance) > 0) {
-            DeviceLight l{};
-            l.normal   = -normalize(f3{dl.direction[0], dl.direction[1], dl.direction[2]});
-            l.radiance = radiance;
-            l.kind     = kLightDirectional;
-            lights.push_back(l);
-            weights.push_back(projected_area * luminance(radiance));
-        }
-    }
-    const f3 environment = {desc.environment[0], desc.environment[1], desc.environment[2]};
-    scene->d.environment        = environment;
-    scene->d.environment_choice = -1;
-    const float integral        = 4.0f * kPi * luminance(environment);
-    if (integral > 0) {
-        DeviceLight l{};
-        l.radiance = environment;
-        l.kind     = kLightEnvironment;
-        scene->d.environment_choice = static_cast<int>(lights.size());
-        lights.push_back(l);
-        weights.push_back(projected_area * integral);
-    }
-    // DiscreteDistribution (src/core/sampling.cpp:109-127) in FP32.
-    std::vector<float> cdf(weights.size() + 1, 0.0f);
-    float maximum = 0;
-    for (float w : weights) {
-        require(std::isfinite(w) && w >= 0, "Distribution weights must be finite and nonnegative");
-        maximum = std::max(maximum, w);
-    }
-    for (size_t i = 0; i < weights.size(); ++i) {
-        cdf[i + 1] = cdf[i] + (maximum > 0 ? weights[i] / maximum : 1.0f);
-    }
-    if (!weights.empty()) {
-        const float integral_cdf = cdf.back();
-        for (auto& v : cdf) {
-            v /= integral_cdf;
-        }
-    }
-    scene->d.light_count = static_cast<uint32_t>(lights.size());
-    scene->lights.allocate(std::max<size_t>(1, lights.size()));
-    scene->light_cdf.allocate(cdf.size());
-    scene->prim_emitter.allocate(emitter_of_prim.size());
-    if (!lights.empty()) {
-        MR_CUDA(cudaMemcpyAsync(scene->lights.ptr, lights.data(), lights.size() * sizeof(DeviceLight),
-                                cudaMemcpyHostToDevice, stream));
-    }
-    MR_CUDA(cudaMemcpyAsync(scene->light_cdf.ptr, cdf.data(), cdf.size() * sizeof(float),
-                            cudaMemcpyHostToDevice, stream));
-    MR_CUDA(cudaMemcpyAsync(scene->prim_emitter.ptr, emitter_of_prim.data(),
-                            emitter_of_prim.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
 
     // ---- media ----
     std::vector<DeviceMedium> media(std::max<uint32_t>(1, desc.medium_count));
@@ -812,8 +895,13 @@ std::unique_ptr<Scene> create_scene(const mr_scene_desc& desc, const mr_bvh_desc
     scene->d.prim_emitter = scene->prim_emitter.ptr;
     scene->d.media        = scene->media.ptr;
     bytes = scene->nodes.bytes() + scene->tris.bytes() + scene->shading.bytes() +
-            scene->ref_nodes.bytes() + scene->ref_order.bytes() + scene->prim_emitter.bytes();
+            scene->ref_nodes.bytes() + scene->ref_order.bytes() + scene->prim_emitter.bytes() +
+            scene->materials.bytes() + scene->lights.bytes() + scene->light_cdf.bytes() +
+            scene->media.bytes();
     scene->device_bytes = bytes;
+    if (scene->two) {
+        publish_two_level(*scene);
+    }
     return scene;
 }
 

@@ -90,9 +90,22 @@ template <typename T> struct DeviceBuffer {
     size_t bytes() const { return count * sizeof(T); }
 };
 
+struct TwoLevel;
+
+// Host copy of the light table: area lights and their fixed weights, directional lights and the
+// environment, whose weights scale with the scene's projected area (LightSampler's constructor,
+// src/render/light.cpp:197-264).
+struct LightTable {
+    std::vector<DeviceLight> lights;
+    std::vector<float>       weights;      // area lights: final; others: per unit projected area
+    std::vector<uint8_t>     scales;       // 1 where the weight scales with the projected area
+};
+
 struct Scene {
     int         device = 0;
     DeviceScene d{};
+    std::unique_ptr<TwoLevel, void (*)(TwoLevel*)> two{nullptr, nullptr};  // two-level scenes only
+    LightTable                                     light_table;
 
     DeviceBuffer<float4>         nodes;
     DeviceBuffer<float4>         tris;
@@ -112,6 +125,22 @@ struct Scene {
     double                   sah_cost      = 0;
     size_t                   device_bytes  = 0;
 };
+
+// Wide (4-child) traversal nodes collapsed from a binary tree, with the binary children each
+// wide node was made from (for refit) and the root's reference and box.
+struct WideTree {
+    DeviceBuffer<float4> nodes;
+    DeviceBuffer<int4>   children;
+    uint32_t             count      = 0;
+    uint32_t             root_count = 0;  // primitives when the root is a leaf (then no nodes)
+    float                lo[3] = {}, hi[3] = {};
+};
+WideTree collapse_tree(const mr_bvh_node* nodes, uint32_t node_count, cudaStream_t stream);
+// Sets kTriLeafEnd on the last triangle slot of every leaf of a binary tree.
+void mark_leaf_ends(const mr_bvh_node* nodes, uint32_t node_count, float4* tris, cudaStream_t stream);
+float determinant3(const float* m);
+// Uploads the light table weighted by the projected area of the world bounds [lo, hi].
+void upload_light_table(Scene& scene, const float* lo, const float* hi, cudaStream_t stream);
 
 // Scene construction (scene.cu). `build` (optional) selects split references for the builder.
 std::unique_ptr<Scene> create_scene(const mr_scene_desc& desc, const mr_bvh_desc* bvh,

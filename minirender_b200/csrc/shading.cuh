@@ -87,21 +87,51 @@ struct SurfaceHit {
     uint32_t instance, triangle, material, prim;
 };
 
+// `slot` is the hit's triangle slot (two-level scenes: its flat primitive id). A two-level scene
+// (TWO and s.two_level) rebuilds the triangle's world vertices and corner normals from its mesh
+// with the flattening's arithmetic, so the hit is the flattened scene's bit for bit.
+template <bool TWO = false>
 __device__ __forceinline__ SurfaceHit surface_hit(const DeviceScene& s, f3 direction,
                                                   uint32_t slot, float b0, float b1, float b2) {
-    const float4* tp = s.tris + 3 * static_cast<size_t>(slot);
-    const float4  a4 = __ldg(tp + 0), b4 = __ldg(tp + 1), c4 = __ldg(tp + 2);
-    const f3      v0 = xyz(a4), v1 = xyz(b4), v2 = xyz(c4);
-    const uint32_t prim  = __float_as_uint(a4.w);
-    const unsigned flags = __float_as_uint(b4.w);
+    f3       v0, v1, v2, m0, m1, m2;
+    uint32_t prim, flags, instance, triangle, material;
+    if (TWO && s.two_level) {
+        prim                        = slot;
+        instance                    = find_instance2(s.instances, s.instance_count, prim);
+        const DeviceInstance2& inst = s.instances[instance];
+        triangle                    = prim - inst.first_prim;
+        material                    = inst.material;
+        flags                       = inst.flags;
+        const mr_mesh_corner* c     = s.mesh_corners + inst.corner_offset + 3 * static_cast<size_t>(triangle);
+        const float*          pos   = s.mesh_positions + 3 * static_cast<size_t>(inst.position_offset);
+        const float*          p0    = pos + 3 * static_cast<size_t>(c[0].position);
+        const float*          p1    = pos + 3 * static_cast<size_t>(c[1].position);
+        const float*          p2    = pos + 3 * static_cast<size_t>(c[2].position);
+        v0 = transform_point(inst.to_world, p0[0], p0[1], p0[2]);
+        v1 = transform_point(inst.to_world, p1[0], p1[1], p1[2]);
+        v2 = transform_point(inst.to_world, p2[0], p2[1], p2[2]);
+        m0 = world_normal(inst.normal_to_world, c[0].normal);
+        m1 = world_normal(inst.normal_to_world, c[1].normal);
+        m2 = world_normal(inst.normal_to_world, c[2].normal);
+    } else {
+        const float4* tp = s.tris + 3 * static_cast<size_t>(slot);
+        const float4  a4 = __ldg(tp + 0), b4 = __ldg(tp + 1), c4 = __ldg(tp + 2);
+        v0    = xyz(a4), v1 = xyz(b4), v2 = xyz(c4);
+        prim  = __float_as_uint(a4.w);
+        flags = __float_as_uint(b4.w);
+        const float4* sp = s.shading + 3 * static_cast<size_t>(prim);
+        const float4  n0 = __ldg(sp + 0), n1 = __ldg(sp + 1), n2 = __ldg(sp + 2);
+        m0       = xyz(n0), m1 = xyz(n1), m2 = xyz(n2);
+        instance = __float_as_uint(n0.w);
+        triangle = __float_as_uint(n1.w);
+        material = __float_as_uint(n2.w);
+    }
     SurfaceHit h;
     f3 geometric = normalize(cross(v1 - v0, v2 - v0));
     if (flags & kTriMirrored) {
         geometric = -geometric;
     }
-    const float4* sp = s.shading + 3 * static_cast<size_t>(prim);
-    const float4  n0 = __ldg(sp + 0), n1 = __ldg(sp + 1), n2 = __ldg(sp + 2);
-    f3 shading = b0 * xyz(n0) + b1 * xyz(n1) + b2 * xyz(n2);
+    f3 shading = b0 * m0 + b1 * m1 + b2 * m2;
     const f3 t0 = b0 * v0, t1 = b1 * v1, t2 = b2 * v2;
     h.position       = t0 + t1 + t2;
     h.position_error = (fabs3(t0) + fabs3(t1) + fabs3(t2)) * (7.0f * kFltEps);
@@ -116,9 +146,9 @@ __device__ __forceinline__ SurfaceHit surface_hit(const DeviceScene& s, f3 direc
     h.geometric_normal = geometric;
     h.shading_normal   = shading;
     h.front_face       = dot(direction, geometric) < 0;
-    h.instance         = __float_as_uint(n0.w);
-    h.triangle         = __float_as_uint(n1.w);
-    h.material         = __float_as_uint(n2.w);
+    h.instance         = instance;
+    h.triangle         = triangle;
+    h.material         = material;
     h.prim             = prim;
     return h;
 }

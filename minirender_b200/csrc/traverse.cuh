@@ -161,9 +161,10 @@ __device__ __forceinline__ bool triangle_test(const RayQuery& q, f3 v0, f3 v1, f
 
 struct TraceResult {
     float    t;
-    uint32_t slot;  // triangle slot in leaf order, kNone for a miss
+    uint32_t slot;  // triangle slot in leaf order (two-level scenes: the primitive), kNone: miss
     uint32_t prim;
     float    a, b, c, det;
+    uint32_t flags;  // two-level scenes: the hit instance's flags
 };
 
 struct TraceCounters {
@@ -322,6 +323,250 @@ __device__ __forceinline__ TraceResult trace(const DeviceScene& s, const RayQuer
                 leaf = node;
                 held = true;
                 pop();
+            }
+        }
+    }
+    return result;
+}
+
+// ---- two-level scenes ----
+
+// The world ray mapped into an instance's object space (same parameter t: the direction is not
+// renormalised), for slab tests against the instance's mesh boxes grown by `margin` on every
+// side. The growth is folded into the origin per axis: o_near/o_far are the origins the near and
+// far planes are measured from. It covers the rounding of this mapping and of the flattening's
+// FP32 world vertices (whose world-space triangles are the ones tested), so a box that a
+// world-space triangle of the instance hits is never culled.
+struct ObjectRay {
+    float o_near[3], o_far[3];
+    float inv_lo[3], inv_hi[3];
+    bool  neg[3];
+};
+
+constexpr float kInstanceMarginScale = 1.9073486328125e-06f;  // 2^-19 = 32 FP32 unit roundoffs
+
+__device__ __forceinline__ void object_ray(const DeviceInstance2& inst, const RayQuery& qw,
+                                           float t_exit, ObjectRay& r) {
+    const float* m = inst.to_object;
+    const f3 o = {fmaf(m[0], qw.o.x, fmaf(m[1], qw.o.y, fmaf(m[2], qw.o.z, m[3]))),
+                  fmaf(m[4], qw.o.x, fmaf(m[5], qw.o.y, fmaf(m[6], qw.o.z, m[7]))),
+                  fmaf(m[8], qw.o.x, fmaf(m[9], qw.o.y, fmaf(m[10], qw.o.z, m[11])))};
+    const f3 d = {fmaf(m[0], qw.d.x, fmaf(m[1], qw.d.y, m[2] * qw.d.z)),
+                  fmaf(m[4], qw.d.x, fmaf(m[5], qw.d.y, m[6] * qw.d.z)),
+                  fmaf(m[8], qw.d.x, fmaf(m[9], qw.d.y, m[10] * qw.d.z))};
+    const float reach  = max3(fabs3(qw.o)) + t_exit * max3(fabs3(qw.d));
+    const float margin = inst.margin_static +
+                         kInstanceMarginScale * (fmaf(inst.a_norm, reach, inst.b_norm));
+    const float lo = 0.99999904632568359375f, hi = 1.00000095367431640625f;  // 1 -+ 2^-20
+    for (int a = 0; a < 3; ++a) {
+        const float c   = comp(d, a);
+        const float inv = 1.0f / c;
+        r.inv_lo[a]     = inv * lo;
+        r.inv_hi[a]     = inv * hi;
+        r.neg[a]        = signbit(c);
+        const float oa  = comp(o, a);
+        r.o_near[a]     = r.neg[a] ? oa - margin : oa + margin;
+        r.o_far[a]      = r.neg[a] ? oa + margin : oa - margin;
+    }
+}
+
+__device__ __forceinline__ float object_slab(const ObjectRay& r, float nx, float fx, float ny, float fy,
+                                             float nz, float fz, float tmin, float tmax) {
+    const float tnx = (nx - r.o_near[0]) * r.inv_lo[0];
+    const float tfx = (fx - r.o_far[0]) * r.inv_hi[0];
+    const float tny = (ny - r.o_near[1]) * r.inv_lo[1];
+    const float tfy = (fy - r.o_far[1]) * r.inv_hi[1];
+    const float tnz = (nz - r.o_near[2]) * r.inv_lo[2];
+    const float tfz = (fz - r.o_far[2]) * r.inv_hi[2];
+    const float enter = fmaxf(fmaxf(tmin, tnx), fmaxf(tny, tnz));
+    const float leave = fminf(fminf(tmax, tfx), fminf(tfy, tfz));
+    return enter <= leave ? enter : __int_as_float(0x7f800000);
+}
+
+// Entry and exit of a world box, or false when the ray misses it within [tmin, tmax].
+__device__ __forceinline__ bool world_box(const RayQuery& q, const float* lo, const float* hi,
+                                          float tmin, float tmax, float& enter, float& leave) {
+    const float nx = ((q.neg[0] ? hi[0] : lo[0]) - q.o.x) * q.inv_lo[0];
+    const float fx = ((q.neg[0] ? lo[0] : hi[0]) - q.o.x) * q.inv_hi[0];
+    const float ny = ((q.neg[1] ? hi[1] : lo[1]) - q.o.y) * q.inv_lo[1];
+    const float fy = ((q.neg[1] ? lo[1] : hi[1]) - q.o.y) * q.inv_hi[1];
+    const float nz = ((q.neg[2] ? hi[2] : lo[2]) - q.o.z) * q.inv_lo[2];
+    const float fz = ((q.neg[2] ? lo[2] : hi[2]) - q.o.z) * q.inv_hi[2];
+    enter = fmaxf(fmaxf(tmin, nx), fmaxf(ny, nz));
+    leave = fminf(fminf(tmax, fx), fminf(fy, fz));
+    return enter <= leave;
+}
+
+// Wide-node children of `node` tested with `test(nx, fx, ny, fy, nz, fz)` (the near/far plane
+// rows picked by `near`), ordered nearest first. Returns the child count hit (<= 4) with refs and
+// entries in r[] / t[].
+template <typename Test>
+__device__ __forceinline__ void wide_children(const float4* nodes, int node, const int near[3],
+                                              Test test, float t[4], int r[4], uint32_t& bounds) {
+    const float4* n   = nodes + 8 * static_cast<size_t>(node);
+    const float4  nx  = __ldg(n + near[0]), fx = __ldg(n + (near[0] ^ 1));
+    const float4  ny  = __ldg(n + near[1]), fy = __ldg(n + (near[1] ^ 1));
+    const float4  nz  = __ldg(n + near[2]), fz = __ldg(n + (near[2] ^ 1));
+    const int4    ref = __ldg(reinterpret_cast<const int4*>(n + 6));
+    bounds += static_cast<uint32_t>(__ldg(reinterpret_cast<const int*>(n + 7)));
+    t[0] = test(nx.x, fx.x, ny.x, fy.x, nz.x, fz.x);
+    t[1] = test(nx.y, fx.y, ny.y, fy.y, nz.y, fz.y);
+    t[2] = test(nx.z, fx.z, ny.z, fy.z, nz.z, fz.z);
+    t[3] = test(nx.w, fx.w, ny.w, fy.w, nz.w, fz.w);
+    r[0] = ref.x, r[1] = ref.y, r[2] = ref.z, r[3] = ref.w;
+    order2(t[0], r[0], t[1], r[1]);
+    order2(t[2], r[2], t[3], r[3]);
+    order2(t[0], r[0], t[2], r[2]);
+    order2(t[1], r[1], t[3], r[3]);
+    order2(t[1], r[1], t[2], r[2]);
+}
+
+// A wide node's or a lone leaf's stack discipline: a stack of (ref, entry) pairs shared by the
+// two levels; entries beyond the current nearest hit are skipped when popped.
+constexpr int kStackSize2 = 3 * 64 * 2 + 3;
+
+// Nearest hit / occlusion in a two-level scene. The instance-level tree is traversed with the
+// world ray; an instance whose world box the ray enters has its mesh tree traversed with the
+// ray mapped into object space, and every candidate triangle is transformed to world space with
+// the flattening's arithmetic (transform_point) and tested with the world ray: the same vertices,
+// ray and test as the flattened scene, so the same hits (ties still go to the lower flat
+// primitive id).
+template <bool ANY_HIT>
+__device__ __forceinline__ TraceResult trace2(const DeviceScene& s, const RayQuery& q, float tmin,
+                                           float tmax, TraceCounters& counters, unsigned& error) {
+    TraceResult result;
+    result.t     = tmax;
+    result.slot  = kNone;
+    result.prim  = kNone;
+    result.flags = 0;
+    if (!s.has_nodes) {
+        return result;
+    }
+    if (!(finite3(q.o) && finite3(q.d))) {
+        error |= kErrorRay;
+        return result;
+    }
+    counters.bounds++;
+    float enter, leave;
+    if (!world_box(q, s.root_lo, s.root_hi, tmin, tmax, enter, leave)) {
+        return result;
+    }
+    int2     stack[kStackSize2];
+    int      sp     = 0;
+    uint32_t visits = 0;
+    const float inf = __int_as_float(0x7f800000);
+    const int near_w[3] = {q.neg[0] ? 1 : 0, q.neg[1] ? 3 : 2, q.neg[2] ? 5 : 4};
+    stack[sp++] = make_int2(s.root, __float_as_int(enter));
+    while (sp > 0) {
+        const int2 top = stack[--sp];
+        if (__int_as_float(top.y) > result.t) {
+            continue;
+        }
+        if (++visits > kMaxVisits) {
+            error |= kErrorVisits;
+            return result;
+        }
+        const int node = top.x;
+        if (node >= 0) {  // instance-level interior node
+            float t[4];
+            int   r[4];
+            wide_children(s.nodes, node, near_w,
+                          [&](float nx, float fx, float ny, float fy, float nz, float fz) {
+                              return slab_near_far(q, nx, fx, ny, fy, nz, fz, tmin, result.t);
+                          },
+                          t, r, counters.bounds);
+            if (sp > kStackSize2 - 4) {
+                error |= kErrorStack;
+                return result;
+            }
+            for (int k = 3; k >= 0; --k) {
+                if (t[k] != inf) {
+                    stack[sp++] = make_int2(r[k], __float_as_int(t[k]));
+                }
+            }
+            continue;
+        }
+        // Instance-level leaf: its instances in order.
+        for (uint32_t item = static_cast<uint32_t>(~node);; ++item) {
+            const uint32_t         word = __ldg(s.tlas_items + item);
+            const DeviceInstance2& inst = s.instances[word & 0x7fffffffu];
+            counters.bounds++;
+            float ienter, ileave;
+            if (world_box(q, inst.lo, inst.hi, tmin, result.t, ienter, ileave)) {
+                ObjectRay ro;
+                object_ray(inst, q, ileave, ro);
+                const int near_o[3] = {ro.neg[0] ? 1 : 0, ro.neg[1] ? 3 : 2, ro.neg[2] ? 5 : 4};
+                const int base = sp;
+                stack[sp++] = make_int2(inst.blas_root, __float_as_int(ienter));
+                while (sp > base) {
+                    const int2 e = stack[--sp];
+                    if (__int_as_float(e.y) > result.t) {
+                        continue;
+                    }
+                    if (++visits > kMaxVisits) {
+                        error |= kErrorVisits;
+                        return result;
+                    }
+                    if (e.x >= 0) {  // mesh-level interior node
+                        float t[4];
+                        int   r[4];
+                        wide_children(s.blas_nodes, e.x, near_o,
+                                      [&](float nx, float fx, float ny, float fy, float nz, float fz) {
+                                          return object_slab(ro, nx, fx, ny, fy, nz, fz, tmin, result.t);
+                                      },
+                                      t, r, counters.bounds);
+                        if (sp > kStackSize2 - 4) {
+                            error |= kErrorStack;
+                            return result;
+                        }
+                        for (int k = 3; k >= 0; --k) {
+                            if (t[k] != inf) {
+                                stack[sp++] = make_int2(r[k], __float_as_int(t[k]));
+                            }
+                        }
+                        continue;
+                    }
+                    // Mesh-level leaf: its triangles, transformed to world space.
+                    for (uint32_t slot = static_cast<uint32_t>(~e.x);; ++slot) {
+                        const float4* tp = s.blas_tris + 3 * static_cast<size_t>(slot);
+                        const float4  a4 = __ldg(tp + 0);
+                        const float4  b4 = __ldg(tp + 1);
+                        const float4  c4 = __ldg(tp + 2);
+                        const f3 v0 = transform_point(inst.to_world, a4.x, a4.y, a4.z);
+                        const f3 v1 = transform_point(inst.to_world, b4.x, b4.y, b4.z);
+                        const f3 v2 = transform_point(inst.to_world, c4.x, c4.y, c4.z);
+                        counters.triangles++;
+                        float tt, ea, eb, ec, det;
+                        if (triangle_test(q, v0, v1, v2, tmin, result.t, tt, ea, eb, ec, det)) {
+                            bool visible = true;
+                            if (inst.flags & kTriSingleSided) {
+                                const float side = dot(q.d, cross(v1 - v0, v2 - v0));
+                                visible = (inst.flags & kTriMirrored) ? side > 0 : side < 0;
+                            }
+                            const uint32_t prim = inst.first_prim + __float_as_uint(a4.w);
+                            if (visible && (tt < result.t || (tt == result.t && prim < result.prim) ||
+                                            result.slot == kNone)) {
+                                result.t     = tt;
+                                result.slot  = prim;
+                                result.prim  = prim;
+                                result.a     = ea;
+                                result.b     = eb;
+                                result.c     = ec;
+                                result.det   = det;
+                                result.flags = inst.flags;
+                                if (ANY_HIT) {
+                                    return result;
+                                }
+                            }
+                        }
+                        if (__float_as_uint(b4.w) & kTriLeafEnd) {
+                            break;
+                        }
+                    }
+                }
+            }
+            if (word & 0x80000000u) {
+                break;
             }
         }
     }

@@ -238,20 +238,37 @@ __global__ void init_rays_kernel(KernelArgs a, WaveInit w) {
 
 // Nearest hit of one extension ray, its material bin (or kNone) and, with media, the
 // free-flight sample over the hit interval.
-template <bool MEDIA>
+// Nearest hit or occlusion in `s`: the flattened traversal, or (TWO) the two-level one when the
+// scene has two levels.
+template <bool ANY_HIT, bool TWO>
+__device__ __forceinline__ TraceResult trace_scene(const DeviceScene& s, const RayQuery& q, float tmin,
+                                                   float tmax, TraceCounters& tc, unsigned& error) {
+    if constexpr (TWO) {
+        if (s.two_level) {
+            return trace2<ANY_HIT>(s, q, tmin, tmax, tc, error);
+        }
+    }
+    return trace<ANY_HIT>(s, q, tmin, tmax, tc, error);
+}
+
+template <bool MEDIA, bool TWO>
 __device__ __forceinline__ uint32_t extend_item(const KernelArgs& a, const DeviceScene& s, uint32_t path,
                                                 bool sorted, TraceCounters& tc, unsigned& error) {
     const float4 o4 = a.st.ray_o[path];
     const float4 d4 = a.st.ray_d[path];
     RayQuery     q;
     q.init(xyz(o4), xyz(d4));
-    const TraceResult r    = trace<false>(s, q, o4.w, d4.w, tc, error);
+    const TraceResult r    = trace_scene<false, TWO>(s, q, o4.w, d4.w, tc, error);
     uint32_t          kind = 0;
     if (r.slot != kNone) {
         a.st.hit[path] = make_float4(r.t, __fdiv_rn(r.a, r.det), __fdiv_rn(r.b, r.det),
                                      __fdiv_rn(r.c, r.det));
         if (sorted) {
-            kind = (__float_as_uint(__ldg(s.tris + 3 * static_cast<size_t>(r.slot) + 1).w) >> 8) & 0xffu;
+            if (TWO && s.two_level) {
+                kind = (r.flags >> 8) & 0xffu;
+            } else {
+                kind = (__float_as_uint(__ldg(s.tris + 3 * static_cast<size_t>(r.slot) + 1).w) >> 8) & 0xffu;
+            }
         }
     }
     a.st.hit_slot[path] = r.slot;
@@ -285,14 +302,14 @@ __device__ __forceinline__ uint32_t extend_item(const KernelArgs& a, const Devic
 
 // Any hit of one shadow segment; adds the contribution (times the media transmittance) when
 // the segment is clear.
-template <bool MEDIA>
+template <bool MEDIA, bool TWO>
 __device__ __forceinline__ void shadow_item(const KernelArgs& a, const DeviceScene& s, uint32_t path,
                                             TraceCounters& tc, unsigned& error) {
     const float4 o4 = a.st.shadow_o[path];
     const float4 d4 = a.st.shadow_d[path];
     RayQuery     q;
     q.init(xyz(o4), xyz(d4));
-    const TraceResult r = trace<true>(s, q, 0.0f, o4.w, tc, error);
+    const TraceResult r = trace_scene<true, TWO>(s, q, 0.0f, o4.w, tc, error);
     if (a.occluded_out) {
         a.occluded_out[path] = r.slot != kNone ? 1 : 0;
     }
@@ -311,9 +328,11 @@ __device__ __forceinline__ void shadow_item(const KernelArgs& a, const DeviceSce
 // before this bounce's shading adds emission, the reference's accumulation order). Warps fetch
 // 32 consecutive items, so only the warp at the boundary mixes the two kinds. 8 resident blocks
 // per SM (<= 64 registers): the traversal is latency bound and more warps hide it. In a
-// multi-job wave (BATCH) every path finds its scene through its segment.
-template <bool MEDIA, bool BATCH>
-__global__ void __launch_bounds__(128, 8) trace_kernel(KernelArgs a) {
+// multi-job wave (BATCH) every path finds its scene through its segment. With two-level scenes
+// in the launch (TWO) the kernel also carries the two-level traversal and runs 5 blocks per SM
+// (<= 102 registers) so that its larger state stays in registers.
+template <bool MEDIA, bool BATCH, bool TWO>
+__global__ void __launch_bounds__(128, TWO ? 5 : 8) trace_kernel(KernelArgs a) {
     BounceCounters* ctr      = a.q.counters + a.bounce;
     const uint32_t  n_ext    = ctr->ext;
     const uint32_t  n_shadow = a.bounce > 0 ? a.q.counters[a.bounce - 1].shadow : 0;
@@ -340,9 +359,9 @@ __global__ void __launch_bounds__(128, 8) trace_kernel(KernelArgs a) {
             const WaveSegment* g = segment_of<BATCH>(a, path);
             unsigned           e = 0;
             if (i < n_ext) {
-                key = extend_item<MEDIA>(a, scene_of<BATCH>(a, g), path, sorted, tc_ext, e);
+                key = extend_item<MEDIA, TWO>(a, scene_of<BATCH>(a, g), path, sorted, tc_ext, e);
             } else {
-                shadow_item<MEDIA>(a, scene_of<BATCH>(a, g), path, tc_shadow, e);
+                shadow_item<MEDIA, TWO>(a, scene_of<BATCH>(a, g), path, tc_shadow, e);
             }
             note_error<BATCH>(g, e, error);
         }
@@ -394,7 +413,7 @@ struct ShadeStats {
     uint32_t shadow_rays = 0, scattering = 0, roulette = 0, medium = 0;
 };
 
-template <bool BATCH>
+template <bool BATCH, bool TWO>
 __device__ ShadeResult shade_surface(const KernelArgs& a, uint32_t path, int bin, ShadeStats& stats,
                                      unsigned& error) {
     const WaveSegment*      g     = segment_of<BATCH>(a, path);
@@ -473,7 +492,7 @@ __device__ ShadeResult shade_surface(const KernelArgs& a, uint32_t path, int bin
     // Surface vertex (src/render/path_tracer.cpp:224-363).
     const float4     h   = a.st.hit[path];
     const uint32_t   slot = a.st.hit_slot[path];
-    const SurfaceHit sh  = surface_hit(s, dir, slot, h.y, h.z, h.w);
+    const SurfaceHit sh  = surface_hit<TWO>(s, dir, slot, h.y, h.z, h.w);
     const DeviceMaterial m = s.materials[sh.material];
     if (m.emission.x > 0 || m.emission.y > 0 || m.emission.z > 0) {
         L += beta * m.emission *
@@ -564,7 +583,7 @@ __device__ ShadeResult shade_surface(const KernelArgs& a, uint32_t path, int bin
     return out;
 }
 
-template <bool BATCH>
+template <bool BATCH, bool TWO>
 __global__ void __launch_bounds__(128) shade_kernel(KernelArgs a) {
     BounceCounters* ctr = a.q.counters + a.bounce;
     uint32_t        prefix[kBinCount + 1];
@@ -590,7 +609,7 @@ __global__ void __launch_bounds__(128) shade_kernel(KernelArgs a) {
             }
             path                 = a.q.bins[bin * static_cast<size_t>(a.capacity) + (i - prefix[bin])];
             unsigned          e  = 0;
-            const ShadeResult r  = shade_surface<BATCH>(a, path, bin, stats, e);
+            const ShadeResult r  = shade_surface<BATCH, TWO>(a, path, bin, stats, e);
             note_error<BATCH>(segment_of<BATCH>(a, path), e, error);
             ext_key              = r.continue_path ? 0u : kNone;
             shadow_key           = r.shadow ? 0u : kNone;
@@ -739,8 +758,9 @@ __global__ void copy_radiance_kernel(const float4* radiance, uint32_t count, flo
 // ---- launch helpers ----
 
 struct LaunchShape {
-    int trace_blocks[2] = {0, 0};
-    int shade_blocks    = 0;
+    int trace_blocks[4]  = {0, 0, 0, 0};  // by media + 2 * two_level
+    int shade_blocks     = 0;
+    int shade_blocks_two = 0;
 };
 
 LaunchShape& launch_shape() {
@@ -752,12 +772,18 @@ LaunchShape& launch_shape() {
         int sms = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, current);
         int per = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, trace_kernel<false, false>, 128, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, trace_kernel<false, false, false>, 128, 0);
         shape.trace_blocks[0] = sms * std::max(1, per);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, trace_kernel<true, false>, 128, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, trace_kernel<true, false, false>, 128, 0);
         shape.trace_blocks[1] = sms * std::max(1, per);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, shade_kernel<false>, 128, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, trace_kernel<false, false, true>, 128, 0);
+        shape.trace_blocks[2] = sms * std::max(1, per);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, trace_kernel<true, false, true>, 128, 0);
+        shape.trace_blocks[3] = sms * std::max(1, per);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, shade_kernel<false, false>, 128, 0);
         shape.shade_blocks = sms * std::max(1, per);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, shade_kernel<false, true>, 128, 0);
+        shape.shade_blocks_two = sms * std::max(1, per);
         device = current;
     }
     return shape;
@@ -980,6 +1006,7 @@ void Engine::run_wave(const Scene& scene, const IntegratorParams& params, const 
     }
     const LaunchShape& shape = launch_shape();
     const bool         media = scene.d.medium_count > 0;
+    const bool         two   = scene.d.two_level != 0;
     KernelTiming&      timing = kernel_timing();
     bool               timed  = false;
     timed = timing.enabled.load();
@@ -1002,17 +1029,23 @@ void Engine::run_wave(const Scene& scene, const IntegratorParams& params, const 
         }
         // The first shadow rays (queued by bounce 0's shading) are traced with bounce 1.
         a.occluded_out = bounce == 1 && init.capture ? init.capture->occluded : nullptr;
-        if (media) {
-            trace_kernel<true, false><<<shape.trace_blocks[1], 128, 0, stream>>>(a);
-        } else {
-            trace_kernel<false, false><<<shape.trace_blocks[0], 128, 0, stream>>>(a);
+        const int variant = (media ? 1 : 0) + (two ? 2 : 0);
+        switch (variant) {
+        case 0: trace_kernel<false, false, false><<<shape.trace_blocks[0], 128, 0, stream>>>(a); break;
+        case 1: trace_kernel<true, false, false><<<shape.trace_blocks[1], 128, 0, stream>>>(a); break;
+        case 2: trace_kernel<false, false, true><<<shape.trace_blocks[2], 128, 0, stream>>>(a); break;
+        default: trace_kernel<true, false, true><<<shape.trace_blocks[3], 128, 0, stream>>>(a); break;
         }
         a.occluded_out = nullptr;
         if (timed) {
             cudaEventRecord(e1, stream);
             events.emplace_back(e0, e1);
         }
-        shade_kernel<false><<<shape.shade_blocks, 128, 0, stream>>>(a);
+        if (two) {
+            shade_kernel<false, true><<<shape.shade_blocks_two, 128, 0, stream>>>(a);
+        } else {
+            shade_kernel<false, false><<<shape.shade_blocks, 128, 0, stream>>>(a);
+        }
         if (bounce == 0 && init.capture) {
             capture_shadow_kernel<<<(init.count + 127) / 128, 128, 0, stream>>>(a, init.capture->rays,
                                                                                 init.capture->has_shadow);
@@ -1042,14 +1075,16 @@ void Engine::run_wave(const Scene& scene, const IntegratorParams& params, const 
 
 void Engine::batch_occupancy(int& trace_blocks_per_sm, int& shade_blocks_per_sm) {
     int a = 0, b = 0, c = 0;
-    MR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, trace_kernel<false, true>, 128, 0));
-    MR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, trace_kernel<true, true>, 128, 0));
-    MR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, shade_kernel<true>, 128, 0));
+    int f = 0;
+    MR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, trace_kernel<false, true, false>, 128, 0));
+    MR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, trace_kernel<true, true, false>, 128, 0));
+    MR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, shade_kernel<true, false>, 128, 0));
+    MR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&f, shade_kernel<true, true>, 128, 0));
     trace_blocks_per_sm = std::max(1, std::min(a, b));
-    shade_blocks_per_sm = std::max(1, c);
+    shade_blocks_per_sm = std::max(1, std::min(c, f));
 }
 
-void Engine::enqueue_batch_paths(const WaveDesc* wave, uint32_t maximum_depth, bool media,
+void Engine::enqueue_batch_paths(const WaveDesc* wave, uint32_t maximum_depth, bool media, bool two,
                                  const BatchShape& shape, Workspace& ws, cudaStream_t stream) {
     if (maximum_depth + 1 > ws.max_bounces || !ws.state.segment) {
         fail(MR_LENGTH_ERROR, "Wave exceeds the workspace capacity");
@@ -1063,16 +1098,30 @@ void Engine::enqueue_batch_paths(const WaveDesc* wave, uint32_t maximum_depth, b
     a.capacity     = static_cast<uint32_t>(ws.capacity);
     a.occluded_out = nullptr;
     a.wave         = wave;
+    // The two-level variants keep fewer blocks resident (more registers per thread): their grid
+    // is capped at what fits, the persistent loop takes the work either way.
+    int trace_blocks = shape.trace_blocks;
+    if (two) {
+        int per = 0;
+        MR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &per, media ? trace_kernel<true, true, true> : trace_kernel<false, true, true>, 128, 0));
+        trace_blocks = std::min(trace_blocks, sms * std::max(1, per));
+    }
     MR_CUDA(cudaMemsetAsync(ws.queues.counters, 0, (maximum_depth + 2) * sizeof(BounceCounters), stream));
     init_batch_kernel<<<sms * 8, 256, 0, stream>>>(a);
     for (uint32_t bounce = 0; bounce <= maximum_depth; ++bounce) {
         a.bounce = bounce;
-        if (media) {
-            trace_kernel<true, true><<<shape.trace_blocks, 128, 0, stream>>>(a);
-        } else {
-            trace_kernel<false, true><<<shape.trace_blocks, 128, 0, stream>>>(a);
+        switch ((media ? 1 : 0) + (two ? 2 : 0)) {
+        case 0: trace_kernel<false, true, false><<<shape.trace_blocks, 128, 0, stream>>>(a); break;
+        case 1: trace_kernel<true, true, false><<<shape.trace_blocks, 128, 0, stream>>>(a); break;
+        case 2: trace_kernel<false, true, true><<<trace_blocks, 128, 0, stream>>>(a); break;
+        default: trace_kernel<true, true, true><<<trace_blocks, 128, 0, stream>>>(a); break;
         }
-        shade_kernel<true><<<shape.shade_blocks, 128, 0, stream>>>(a);
+        if (two) {
+            shade_kernel<true, true><<<shape.shade_blocks, 128, 0, stream>>>(a);
+        } else {
+            shade_kernel<true, false><<<shape.shade_blocks, 128, 0, stream>>>(a);
+        }
     }
     MR_CUDA(cudaGetLastError());
 }

@@ -165,7 +165,7 @@ class Engine {
     // (`wave`): camera paths of every segment and up to maximum_depth + 1 bounces; radiance stays
     // per path. The launch sequence depends only on its arguments, so it can be captured once in
     // a CUDA graph and replayed for every wave of the same depth.
-    static void enqueue_batch_paths(const WaveDesc* wave, uint32_t maximum_depth, bool media,
+    static void enqueue_batch_paths(const WaveDesc* wave, uint32_t maximum_depth, bool media, bool two,
                                     const BatchShape& shape, Workspace& ws, cudaStream_t stream);
 
     // Enqueues the per-pixel resolve of a wave's radiance into each job's accumulator and image.
