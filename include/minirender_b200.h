@@ -87,7 +87,16 @@ typedef struct mr_camera {
     float focus_distance;
 } mr_camera;
 
-/* Material (include/minirender/scene/scene.hpp:113-136), the fields the offline path reads. */
+/* TextureFilter (include/minirender/core/texture.hpp:14). */
+typedef enum mr_texture_filter {
+    MR_FILTER_NEAREST   = 0,
+    MR_FILTER_BILINEAR  = 1,
+    MR_FILTER_TRILINEAR = 2
+} mr_texture_filter;
+
+/* Material (include/minirender/scene/scene.hpp:113-136), the fields the offline path reads.
+ * Textures are 1-based indices into mr_scene_desc.textures, 0 = none (RenderInstance resolves
+ * the material's texture ids, include/minirender/scene/scene.hpp:201-209). */
 typedef struct mr_material {
     uint32_t kind; /* mr_material_kind */
     float    base_color[3];
@@ -95,7 +104,20 @@ typedef struct mr_material {
     float    roughness;
     float    ior;
     uint32_t double_sided;
+    uint32_t base_color_texture; /* multiplies base_color after clamping to [0,1] */
+    uint32_t texture_filter;     /* mr_texture_filter of both textures */
+    uint32_t normal_texture;     /* tangent-space normals decoded in the triangle's UV frame */
+    float    normal_scale;       /* xy scale of the decoded normal; <= 0 disables the map */
+    uint32_t normal_flip_y;
 } mr_material;
+
+/* A decoded texture (TextureAsset's data, include/minirender/scene/scene.hpp:148-154): linear
+ * RGB, width * height * 3 floats, row 0 at the top of the image. */
+typedef struct mr_texture {
+    const float* rgb;
+    uint32_t     width;
+    uint32_t     height;
+} mr_texture;
 
 /* MeshCorner (include/minirender/scene/scene.hpp:33-37): 24 bytes. */
 typedef struct mr_mesh_corner {
@@ -138,7 +160,7 @@ typedef struct mr_medium_region {
     uint32_t enabled;
 } mr_medium_region;
 
-/* SceneSnapshot (include/minirender/scene/scene.hpp:220-230) without textures. */
+/* SceneSnapshot (include/minirender/scene/scene.hpp:220-230). */
 typedef struct mr_scene_desc {
     mr_camera                   camera;
     float                       environment[3];
@@ -152,6 +174,11 @@ typedef struct mr_scene_desc {
     uint32_t                    directional_light_count;
     const mr_medium_region*     media;
     uint32_t                    medium_count;
+    const mr_texture*           textures;
+    uint32_t                    texture_count;
+    uint32_t                    environment_texture;  /* 1-based lat-long map, 0 = none */
+    float                       environment_strength; /* scales the map (not the constant) */
+    float                       environment_rotation_degrees; /* about +Y, right-handed */
 } mr_scene_desc;
 
 /* SceneBvh::Node (include/minirender/render/bvh.hpp:81-86), the reference's flat node layout.

@@ -51,7 +51,17 @@ class Camera(C.Structure):
 
 class Material(C.Structure):
     _fields_ = [("kind", C.c_uint32), ("base_color", f3), ("emission", f3),
-                ("roughness", C.c_float), ("ior", C.c_float), ("double_sided", C.c_uint32)]
+                ("roughness", C.c_float), ("ior", C.c_float), ("double_sided", C.c_uint32),
+                ("base_color_texture", C.c_uint32), ("texture_filter", C.c_uint32),
+                ("normal_texture", C.c_uint32), ("normal_scale", C.c_float),
+                ("normal_flip_y", C.c_uint32)]
+
+
+class Texture(C.Structure):
+    _fields_ = [("rgb", C.POINTER(C.c_float)), ("width", C.c_uint32), ("height", C.c_uint32)]
+
+
+TEXTURE_FILTERS = {"nearest": 0, "bilinear": 1, "trilinear": 2}
 
 
 class MeshCorner(C.Structure):
@@ -84,7 +94,10 @@ class SceneDesc(C.Structure):
                 ("instances", C.POINTER(Instance)), ("instance_count", C.c_uint32),
                 ("directional_lights", C.POINTER(DirectionalLight)),
                 ("directional_light_count", C.c_uint32),
-                ("media", C.POINTER(MediumRegion)), ("medium_count", C.c_uint32)]
+                ("media", C.POINTER(MediumRegion)), ("medium_count", C.c_uint32),
+                ("textures", C.POINTER(Texture)), ("texture_count", C.c_uint32),
+                ("environment_texture", C.c_uint32), ("environment_strength", C.c_float),
+                ("environment_rotation_degrees", C.c_float)]
 
 
 class BvhNode(C.Structure):

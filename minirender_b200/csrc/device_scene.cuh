@@ -66,6 +66,18 @@ struct DeviceMaterial {
     float    ior;
     uint32_t kind;
     uint32_t double_sided;
+    int      base_texture;    // index into the scene's textures, -1 none
+    int      normal_texture;  // index into the scene's textures, -1 none
+    uint32_t filter;          // mr_texture_filter
+    float    normal_scale;
+    uint32_t normal_flip_y;
+};
+
+// Level 0 of a texture: width x height texels (linear RGB in xyz) from `offset` of the scene's
+// texel array, row 0 at the top of the image.
+struct DeviceTexture {
+    uint32_t width, height;
+    uint64_t offset;
 };
 
 enum LightKindCode : uint32_t { kLightArea = 0, kLightDirectional = 1, kLightEnvironment = 2 };
@@ -157,6 +169,23 @@ struct DeviceScene {
     // its own object-space tree in blas_nodes over object-space triangle slots in blas_tris
     // ([0] = v0.xyz + triangle index within the mesh, [1] = v1.xyz + kTriLeafEnd, [2] = v2.xyz).
     // The meshes' positions and corners stay resident for shading.
+    // Textures (any material or the environment uses one): texels, per-texture records, and for
+    // flattened scenes the corner UVs of every primitive (3 per primitive, null without textures).
+    const float4*          texels;
+    const DeviceTexture*   textures;
+    const float2*          uvs;
+    // Environment map: texture index (-1: constant environment only), strength, rotation about
+    // +Y in radians, and its importance distribution over a grid of env_w x env_h texels (a mip
+    // level): the row marginal CDF (env_h + 1 entries), each row's conditional CDF (env_w + 1
+    // entries per row) and each row's texel solid angle; env_uniform: sample the sphere
+    // uniformly (no map, zero strength, or a map without radiance).
+    int                    env_texture;
+    float                  env_strength, env_rotation;
+    int                    env_uniform;
+    uint32_t               env_w, env_h;
+    const float*           env_row_cdf;
+    const float*           env_col_cdf;
+    const float*           env_solid_angle;
     int                    two_level;
     uint32_t               instance_count;
     const DeviceInstance2* instances;

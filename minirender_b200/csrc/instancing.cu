@@ -534,7 +534,9 @@ void publish_two_level(Scene& scene) {
     scene.device_bytes = t.instances.bytes() + t.tlas_nodes.bytes() + t.tlas_items.bytes() + t.blas_nodes.bytes() +
                          t.blas_tris.bytes() + t.positions.bytes() + t.corners.bytes() +
                          scene.prim_emitter.bytes() + scene.materials.bytes() + scene.lights.bytes() +
-                         scene.light_cdf.bytes() + scene.media.bytes();
+                         scene.light_cdf.bytes() + scene.media.bytes() + scene.texels.bytes() +
+                         scene.texture_table.bytes() + scene.env_row_cdf.bytes() + scene.env_col_cdf.bytes() +
+                         scene.env_solid_angle.bytes();
     for (const auto& m : t.mesh) {
         scene.device_bytes += m.nodes.bytes() + m.order.bytes();
     }

@@ -49,7 +49,7 @@ __device__ __forceinline__ uint32_t find_instance(const DeviceInstance* instance
 __global__ void flatten_kernel(const float* positions, const mr_mesh_corner* corners,
                                const DeviceInstance* instances, uint32_t instance_count,
                                uint32_t prim_count, float4* world, float4* shading, float4* lo,
-                               float4* hi, float4* centroid, unsigned* error) {
+                               float4* hi, float4* centroid, unsigned* error, float2* uvs) {
     const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= prim_count) {
         return;
@@ -64,6 +64,9 @@ __global__ void flatten_kernel(const float* positions, const mr_mesh_corner* cor
         const float*          q      = positions + 3 * (static_cast<size_t>(inst.position_offset) + corner.position);
         v[c] = transform_point(inst.object_to_world, q[0], q[1], q[2]);
         n[c] = world_normal(inst.normal_to_world, corner.normal);
+        if (uvs) {
+            uvs[3 * static_cast<size_t>(p) + c] = make_float2(corner.uv[0], corner.uv[1]);
+        }
     }
     if (!finite3(v[0]) || !finite3(v[1]) || !finite3(v[2])) {
         atomicOr(error, 1u);
@@ -461,7 +464,7 @@ void upload_light_table(Scene& scene, const float* lo, const float* hi, cudaStre
 // The host light table and the primitive -> emitter map: area lights in instance and triangle
 // order, then directional lights, then the constant environment.
 void build_light_table(Scene& scene, const mr_scene_desc& desc, const std::vector<uint32_t>& first_prim,
-                       cudaStream_t stream) {
+                       double map_integral, cudaStream_t stream) {
     LightTable&           t     = scene.light_table;
     const uint32_t        prims = scene.d.primitive_count;
     std::vector<uint32_t> emitter_of_prim(std::max<uint32_t>(1, prims), kNone);
@@ -517,7 +520,7 @@ void build_light_table(Scene& scene, const mr_scene_desc& desc, const std::vecto
     const f3 environment        = {desc.environment[0], desc.environment[1], desc.environment[2]};
     scene.d.environment         = environment;
     scene.d.environment_choice  = -1;
-    const float integral        = 4.0f * kPi * luminance(environment);
+    const float integral        = 4.0f * kPi * luminance(environment) + static_cast<float>(map_integral);
     if (integral > 0) {
         DeviceLight l{};
         l.radiance                 = environment;
@@ -719,10 +722,13 @@ std::unique_ptr<Scene> create_scene(const mr_scene_desc& desc, const mr_bvh_desc
         error.allocate(1);
         MR_CUDA(cudaMemsetAsync(error.ptr, 0, sizeof(uint32_t), stream));
         if (prims) {
+            if (desc.texture_count) {  // corner UVs for texture lookups and normal maps
+                scene->uvs.allocate(3ull * prims);
+            }
             flatten_kernel<<<(prims + 255) / 256, 256, 0, stream>>>(
                 positions.ptr, corners.ptr, reinterpret_cast<const DeviceInstance*>(instance_buffer.ptr),
                 desc.instance_count, prims, world.ptr, scene->shading.ptr, lo.ptr, hi.ptr, centroid.ptr,
-                error.ptr);
+                error.ptr, scene->uvs.ptr);
             MR_CUDA(cudaGetLastError());
         }
         uint32_t flatten_error = 0;
@@ -834,16 +840,23 @@ std::unique_ptr<Scene> create_scene(const mr_scene_desc& desc, const mr_bvh_desc
     std::vector<DeviceMaterial> materials(std::max<uint32_t>(1, desc.material_count));
     for (uint32_t i = 0; i < desc.material_count; ++i) {
         const mr_material& m = desc.materials[i];
+        require(m.base_color_texture <= desc.texture_count && m.normal_texture <= desc.texture_count,
+                "Material references missing texture");
+        require(m.texture_filter <= MR_FILTER_TRILINEAR, "Unknown texture filter");
+        require(std::isfinite(m.normal_scale), "Normal scale must be finite");
         materials[i] = {{m.base_color[0], m.base_color[1], m.base_color[2]},
                         {m.emission[0], m.emission[1], m.emission[2]},
-                        m.roughness * m.roughness, m.ior, m.kind, m.double_sided};
+                        m.roughness * m.roughness, m.ior, m.kind, m.double_sided,
+                        static_cast<int>(m.base_color_texture) - 1, static_cast<int>(m.normal_texture) - 1,
+                        m.texture_filter, m.normal_scale, m.normal_flip_y};
     }
     scene->materials.allocate(materials.size());
     MR_CUDA(cudaMemcpyAsync(scene->materials.ptr, materials.data(), materials.size() * sizeof(DeviceMaterial),
                             cudaMemcpyHostToDevice, stream));
 
     // ---- lights (LightSampler constructor, src/render/light.cpp:197-264) ----
-    build_light_table(*scene, desc, first_prim, stream);
+    upload_textures(*scene, desc, stream);
+    build_light_table(*scene, desc, first_prim, prepare_environment(*scene, desc, stream), stream);
     if (scene->two) {
         upload_light_table(*scene, scene->two->world_lo, scene->two->world_hi, stream);
     } else {
@@ -894,10 +907,12 @@ std::unique_ptr<Scene> create_scene(const mr_scene_desc& desc, const mr_bvh_desc
     scene->d.light_cdf    = scene->light_cdf.ptr;
     scene->d.prim_emitter = scene->prim_emitter.ptr;
     scene->d.media        = scene->media.ptr;
+    scene->d.uvs          = scene->uvs.ptr;
     bytes = scene->nodes.bytes() + scene->tris.bytes() + scene->shading.bytes() +
             scene->ref_nodes.bytes() + scene->ref_order.bytes() + scene->prim_emitter.bytes() +
             scene->materials.bytes() + scene->lights.bytes() + scene->light_cdf.bytes() +
-            scene->media.bytes();
+            scene->media.bytes() + scene->uvs.bytes() + scene->texels.bytes() + scene->texture_table.bytes() +
+            scene->env_row_cdf.bytes() + scene->env_col_cdf.bytes() + scene->env_solid_angle.bytes();
     scene->device_bytes = bytes;
     if (scene->two) {
         publish_two_level(*scene);

@@ -115,6 +115,10 @@ struct Scene {
     DeviceBuffer<float>          light_cdf;
     DeviceBuffer<uint32_t>       prim_emitter;
     DeviceBuffer<DeviceMedium>   media;
+    DeviceBuffer<float4>         texels;
+    DeviceBuffer<DeviceTexture>  texture_table;
+    DeviceBuffer<float2>         uvs;  // flattened scenes with textures: corner UVs per primitive
+    DeviceBuffer<float>          env_row_cdf, env_col_cdf, env_solid_angle;
 
     // Reference-layout BVH (mr_bvh_node + order) kept on the device for export and SAH.
     DeviceBuffer<mr_bvh_node> ref_nodes;
@@ -139,6 +143,11 @@ WideTree collapse_tree(const mr_bvh_node* nodes, uint32_t node_count, cudaStream
 // Sets kTriLeafEnd on the last triangle slot of every leaf of a binary tree.
 void mark_leaf_ends(const mr_bvh_node* nodes, uint32_t node_count, float4* tris, cudaStream_t stream);
 float determinant3(const float* m);
+// Validates and uploads the scene's textures (environment.cu).
+void upload_textures(Scene& scene, const mr_scene_desc& desc, cudaStream_t stream);
+// The environment map's device fields and importance distribution; returns the map's luminance
+// integral (strength x the integral over level 0) for light selection (environment.cu).
+double prepare_environment(Scene& scene, const mr_scene_desc& desc, cudaStream_t stream);
 // Uploads the light table weighted by the projected area of the world bounds [lo, hi].
 void upload_light_table(Scene& scene, const float* lo, const float* hi, cudaStream_t stream);
 

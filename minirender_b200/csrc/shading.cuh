@@ -35,6 +35,12 @@ __device__ __forceinline__ f3 sample_sphere(float ux, float uy) {
     return {radius * c, radius * s, z};
 }
 
+}  // namespace mr
+
+#include "textures.cuh"
+
+namespace mr {
+
 __device__ __forceinline__ f3 sample_cosine_hemisphere(float ux, float uy) {
     float dx, dy;
     sample_disk(ux, uy, dx, dy);
@@ -83,6 +89,7 @@ struct SurfaceHit {
     f3       position_error;
     f3       geometric_normal;
     f3       shading_normal;
+    float    u, v;  // interpolated corner UVs (0 when the scene has no textures)
     bool     front_face;
     uint32_t instance, triangle, material, prim;
 };
@@ -94,6 +101,7 @@ template <bool TWO = false>
 __device__ __forceinline__ SurfaceHit surface_hit(const DeviceScene& s, f3 direction,
                                                   uint32_t slot, float b0, float b1, float b2) {
     f3       v0, v1, v2, m0, m1, m2;
+    float2   c0 = make_float2(0, 0), c1 = c0, c2 = c0;  // corner UVs
     uint32_t prim, flags, instance, triangle, material;
     if (TWO && s.two_level) {
         prim                        = slot;
@@ -113,6 +121,11 @@ __device__ __forceinline__ SurfaceHit surface_hit(const DeviceScene& s, f3 direc
         m0 = world_normal(inst.normal_to_world, c[0].normal);
         m1 = world_normal(inst.normal_to_world, c[1].normal);
         m2 = world_normal(inst.normal_to_world, c[2].normal);
+        if (s.textures) {
+            c0 = make_float2(c[0].uv[0], c[0].uv[1]);
+            c1 = make_float2(c[1].uv[0], c[1].uv[1]);
+            c2 = make_float2(c[2].uv[0], c[2].uv[1]);
+        }
     } else {
         const float4* tp = s.tris + 3 * static_cast<size_t>(slot);
         const float4  a4 = __ldg(tp + 0), b4 = __ldg(tp + 1), c4 = __ldg(tp + 2);
@@ -125,6 +138,11 @@ __device__ __forceinline__ SurfaceHit surface_hit(const DeviceScene& s, f3 direc
         instance = __float_as_uint(n0.w);
         triangle = __float_as_uint(n1.w);
         material = __float_as_uint(n2.w);
+        if (s.uvs) {
+            c0 = __ldg(s.uvs + 3 * static_cast<size_t>(prim));
+            c1 = __ldg(s.uvs + 3 * static_cast<size_t>(prim) + 1);
+            c2 = __ldg(s.uvs + 3 * static_cast<size_t>(prim) + 2);
+        }
     }
     SurfaceHit h;
     f3 geometric = normalize(cross(v1 - v0, v2 - v0));
@@ -141,6 +159,14 @@ __device__ __forceinline__ SurfaceHit surface_hit(const DeviceScene& s, f3 direc
         shading = normalize(shading);
         if (dot(shading, geometric) < 0) {
             shading = -shading;
+        }
+    }
+    h.u = b0 * c0.x + b1 * c1.x + b2 * c2.x;
+    h.v = b0 * c0.y + b1 * c1.y + b2 * c2.y;
+    if (s.textures) {
+        const DeviceMaterial& m = s.materials[material];
+        if (m.normal_texture >= 0 && m.normal_scale > 0) {
+            shading = apply_normal_map(s, m, shading, geometric, v0, v1, v2, c0, c1, c2, h.u, h.v);
         }
     }
     h.geometric_normal = geometric;
@@ -237,8 +263,12 @@ struct Bsdf {  // Bsdf (bsdf.cpp:122-277) without cloth, subsurface and energy c
     float    alpha, eta_i, eta_t;
     uint32_t kind;
 
-    __device__ __forceinline__ void init(const DeviceMaterial& m, bool front_face) {
-        color = m.base_color;
+    // color = base_color * clamp(texture colour, 0, 1) (bsdf.cpp:122-141).
+    __device__ __forceinline__ void init(const DeviceMaterial& m, bool front_face,
+                                         f3 texture_color = make(1.0f, 1.0f, 1.0f)) {
+        color = m.base_color * make(fminf(fmaxf(texture_color.x, 0.0f), 1.0f),
+                                    fminf(fmaxf(texture_color.y, 0.0f), 1.0f),
+                                    fminf(fmaxf(texture_color.z, 0.0f), 1.0f));
         alpha = m.alpha;
         eta_i = front_face ? 1.0f : m.ior;
         eta_t = front_face ? m.ior : 1.0f;
@@ -380,7 +410,7 @@ __device__ __forceinline__ int select_light(const DeviceScene& s, float u, float
     return index;
 }
 
-// LightSampler::sample (light.cpp:266-321), constant environment only.
+// LightSampler::sample (light.cpp:266-321).
 __device__ __forceinline__ bool sample_light(const DeviceScene& s, f3 reference, float light_u,
                                              float ux, float uy, LightSample& out) {
     if (s.light_count == 0) {
@@ -398,10 +428,10 @@ __device__ __forceinline__ bool sample_light(const DeviceScene& s, f3 reference,
         return true;
     }
     if (light.kind == kLightEnvironment) {
-        out.direction   = sample_sphere(ux, uy);
-        out.radiance    = light.radiance;
+        float density;
+        out.direction   = sample_environment(s, ux, uy, density, out.radiance);
         out.distance    = INFINITY;
-        out.probability = mass * (1.0f / (4.0f * kPi));
+        out.probability = mass * density;
         out.discrete    = false;
         return true;
     }
@@ -443,13 +473,13 @@ __device__ __forceinline__ float area_pdf(const DeviceScene& s, f3 reference, ui
     return mass * area_density(reference, position, light.normal, light.area);
 }
 
-__device__ __forceinline__ float environment_pdf(const DeviceScene& s) {  // light.cpp:336-340
+__device__ __forceinline__ float environment_pdf(const DeviceScene& s, f3 direction) {  // light.cpp:336-340
     if (s.environment_choice < 0) {
         return 0.0f;
     }
     const float mass = __ldg(s.light_cdf + s.environment_choice + 1) -
                        __ldg(s.light_cdf + s.environment_choice);
-    return mass * (1.0f / (4.0f * kPi));
+    return mass * environment_density(s, direction);
 }
 
 // The shadow segment of PathTracer::shadow_transmittance (path_tracer.cpp:126-151): both ends

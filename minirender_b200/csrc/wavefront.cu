@@ -432,8 +432,8 @@ __device__ ShadeResult shade_surface(const KernelArgs& a, uint32_t path, int bin
     ShadeResult             out{false, false};
 
     if (bin == kBinMiss) {
-        L += beta * s.environment *
-             emission_weight(p, depth, previous_delta, prev4.w, environment_pdf(s));
+        L += beta * environment_radiance(s, dir) *
+             emission_weight(p, depth, previous_delta, prev4.w, environment_pdf(s, dir));
         a.st.radiance[path] = f4(L, 0);
         return out;
     }
@@ -512,7 +512,9 @@ __device__ ShadeResult shade_surface(const KernelArgs& a, uint32_t path, int bin
     frame.init(normal);
     const f3 wo = frame.to_local(wo_world);
     Bsdf     bsdf;
-    bsdf.init(m, sh.front_face);
+    bsdf.init(m, sh.front_face,
+              m.base_texture >= 0 ? texture_sample(s, m.base_texture, sh.u, sh.v, m.filter)
+                                  : make(1.0f, 1.0f, 1.0f));  // path_tracer.cpp:279-282
     const float light_u   = rng.next_1d();
     const float sux       = rng.next_1d();
     const float suy       = rng.next_1d();

@@ -91,3 +91,234 @@ def write_exr(path: str, rgb: np.ndarray):
         for y in range(height):
             f.write(struct.pack("<ii", y, line_bytes))
             f.write(planes[y].tobytes())
+
+
+# ---- texture input (Image::read, src/core/raster_io.cpp:40-113) ----
+
+def srgb_to_linear(encoded: np.ndarray) -> np.ndarray:
+    """srgb_to_linear (src/core/image.cpp:34-40) in float32: nonfinite -> 0, negative -> 0."""
+    x = np.asarray(encoded, F32)
+    x = np.where(np.isfinite(x), np.maximum(x, F32(0)), F32(0)).astype(F32)
+    powered = np.power(((x + F32(0.055)) / F32(1.055)).astype(F32), F32(2.4)).astype(F32)
+    return np.where(x <= F32(0.04045), (x / F32(12.92)).astype(F32), powered).astype(F32)
+
+
+def _paeth(a, b, c):
+    p = a + b - c
+    pa, pb, pc = np.abs(p - a), np.abs(p - b), np.abs(p - c)
+    return np.where((pa <= pb) & (pa <= pc), a, np.where(pb <= pc, b, c))
+
+
+def _unfilter(raw: bytes, height: int, stride: int, bpp: int) -> np.ndarray:
+    """PNG scanline filters (types 0-4) undone; (height, stride) bytes."""
+    data = np.frombuffer(raw, np.uint8)
+    if data.size != height * (stride + 1):
+        raise ValueError("PNG image data has the wrong size")
+    rows = data.reshape(height, stride + 1)
+    out = np.zeros((height, stride), np.int32)
+    previous = np.zeros(stride, np.int32)
+    for y in range(height):
+        kind, line = rows[y, 0], rows[y, 1:].astype(np.int32)
+        if kind == 0:
+            cur = line
+        elif kind == 2:
+            cur = (line + previous) & 0xFF
+        elif kind == 1:  # Sub: a running sum per byte of the pixel
+            padded = np.zeros(((stride + bpp - 1) // bpp) * bpp, np.int32)
+            padded[:stride] = line
+            cur = (np.cumsum(padded.reshape(-1, bpp), axis=0).reshape(-1) & 0xFF)[:stride]
+        elif kind in (3, 4):  # Average, Paeth: pixel by pixel, each pixel's bytes at once
+            cur = np.zeros(stride, np.int32)
+            left = np.zeros(bpp, np.int32)
+            upleft = np.zeros(bpp, np.int32)
+            for i in range(0, stride, bpp):
+                up = previous[i:i + bpp]
+                k = up.size
+                if kind == 3:
+                    pred = (left[:k] + up) >> 1
+                else:
+                    pred = _paeth(left[:k], up, upleft[:k])
+                cur[i:i + k] = (line[i:i + k] + pred) & 0xFF
+                left, upleft = cur[i:i + k], up
+        else:
+            raise ValueError("PNG uses an unknown filter type")
+        out[y] = cur
+        previous = cur
+    return out
+
+
+def read_png(path: str) -> np.ndarray:
+    """RGB samples of a PNG scaled to [0, 1] as stb_image delivers three channels (grey
+    replicated, alpha dropped, palette expanded; 1/2/4-bit grey scaled to 8 bits): (height,
+    width, 3) float32. Interlaced (Adam7) files are rejected."""
+    data = open(path, "rb").read()
+    if data[:8] != b"\x89PNG\r\n\x1a\n":
+        raise ValueError("Unsupported or corrupt texture image")
+    pos, idat, palette, header = 8, [], None, None
+    while pos + 8 <= len(data):
+        n = struct.unpack(">I", data[pos:pos + 4])[0]
+        kind, body = data[pos + 4:pos + 8], data[pos + 8:pos + 8 + n]
+        if kind == b"IHDR":
+            header = struct.unpack(">IIBBBBB", body[:13])
+        elif kind == b"PLTE":
+            palette = np.frombuffer(body, np.uint8).reshape(-1, 3)
+        elif kind == b"IDAT":
+            idat.append(body)
+        elif kind == b"IEND":
+            break
+        pos += 12 + n
+    if header is None:
+        raise ValueError("Unsupported or corrupt texture image")
+    width, height, depth, color, _, _, interlace = header
+    if width == 0 or height == 0 or width > 16384 or height > 16384 or width * height > 64 * 1024 * 1024:
+        raise ValueError("Texture exceeds the 64-megapixel budget")
+    if interlace:
+        raise ValueError("Interlaced PNG textures are not supported")
+    channels = {0: 1, 2: 3, 3: 1, 4: 2, 6: 4}.get(color)
+    if channels is None or depth not in (1, 2, 4, 8, 16):
+        raise ValueError("Unsupported or corrupt texture image")
+    bits = channels * depth
+    stride = (width * bits + 7) // 8
+    rows = _unfilter(zlib.decompress(b"".join(idat)), height, stride, max(1, bits // 8))
+    if depth == 16:
+        samples = (rows[:, 0::2] << 8 | rows[:, 1::2]).reshape(height, width, channels)
+        scale = F32(65535)
+    elif depth == 8:
+        samples = rows.reshape(height, width, channels)
+        scale = F32(255)
+    else:
+        per = 8 // depth
+        shifts = np.arange(per - 1, -1, -1) * depth
+        unpacked = ((rows[:, :, None] >> shifts) & ((1 << depth) - 1)).reshape(height, -1)[:, :width]
+        samples = unpacked.reshape(height, width, 1)
+        if color == 0:  # grey scaled to 8 bits
+            samples = samples * (255 // ((1 << depth) - 1))
+        scale = F32(255)
+    if color == 3:
+        if palette is None:
+            raise ValueError("Unsupported or corrupt texture image")
+        rgb = palette[np.minimum(samples[..., 0], len(palette) - 1)].astype(np.int32)
+    elif color in (0, 4):
+        rgb = np.repeat(samples[..., :1], 3, axis=2)
+    else:
+        rgb = samples[..., :3]
+    return (rgb.astype(F32) / scale).astype(F32)
+
+
+def _half_to_float(h: np.ndarray) -> np.ndarray:
+    return h.astype("<u2").view("<f2").astype(F32)
+
+
+def read_exr(path: str) -> np.ndarray:
+    """(height, width, 3) float32 RGB of a scanline OpenEXR file: HALF or FLOAT channels R, G, B
+    (or Y, replicated), compression NONE, ZIPS or ZIP."""
+    data = open(path, "rb").read()
+    magic, version = struct.unpack("<ii", data[:8])
+    if magic != 20000630 or (version & 0xFF) != 2 or version & 0x200:
+        raise ValueError("Only scanline OpenEXR files are supported")
+    pos, attrs = 8, {}
+    while data[pos] != 0:
+        end = data.index(b"\x00", pos)
+        name = data[pos:end].decode()
+        tend = data.index(b"\x00", end + 1)
+        size = struct.unpack("<i", data[tend + 1:tend + 5])[0]
+        attrs[name] = data[tend + 5:tend + 5 + size]
+        pos = tend + 5 + size
+    pos += 1
+    x0, y0, x1, y1 = struct.unpack("<iiii", attrs["dataWindow"])
+    width, height = x1 - x0 + 1, y1 - y0 + 1
+    compression = attrs["compression"][0]
+    lines = {0: 1, 2: 1, 3: 16}.get(compression)
+    if lines is None:
+        raise ValueError("EXR compression must be NONE, ZIPS or ZIP")
+    chlist, channels, k = attrs["channels"], [], 0
+    while chlist[k] != 0:
+        end = chlist.index(b"\x00", k)
+        name = chlist[k:end].decode()
+        kind = struct.unpack("<i", chlist[end + 1:end + 5])[0]
+        channels.append((name, kind))
+        k = end + 17
+    sizes = {1: 2, 2: 4}
+    if any(kind not in sizes for _, kind in channels):
+        raise ValueError("EXR channels must be HALF or FLOAT")
+    blocks = (height + lines - 1) // lines
+    offsets = struct.unpack(f"<{blocks}Q", data[pos:pos + 8 * blocks])
+    planes = {name: np.zeros((height, width), F32) for name, _ in channels}
+    for off in offsets:
+        y, size = struct.unpack("<ii", data[off:off + 8])
+        chunk = data[off + 8:off + 8 + size]
+        n = min(lines, y1 + 1 - y)
+        expected = n * width * sum(sizes[kind] for _, kind in channels)
+        if compression and size < expected:
+            raw = np.frombuffer(zlib.decompress(chunk), np.uint8).astype(np.int32)
+            raw = np.cumsum(np.concatenate([raw[:1], raw[1:] - 128])) & 0xFF  # predictor
+            half = (raw.size + 1) // 2
+            interleaved = np.empty(raw.size, np.uint8)
+            interleaved[0::2], interleaved[1::2] = raw[:half], raw[half:]
+            chunk = interleaved.tobytes()
+        at = 0
+        for line in range(n):
+            for name, kind in channels:
+                count = width * sizes[kind]
+                values = np.frombuffer(chunk[at:at + count], "<u2" if kind == 1 else "<f4")
+                planes[name][y - y0 + line] = _half_to_float(values) if kind == 1 else values
+                at += count
+    if all(c in planes for c in "RGB"):
+        return np.stack([planes["R"], planes["G"], planes["B"]], axis=2)
+    if "Y" in planes:
+        return np.repeat(planes["Y"][..., None], 3, axis=2)
+    raise ValueError("EXR texture needs R, G and B or Y channels")
+
+
+def read_hdr(path: str) -> np.ndarray:
+    """(height, width, 3) float32 RGB of a Radiance RGBE file (flat or run-length scanlines),
+    converted as stb_image converts it (mantissa x 2^(exponent - 136))."""
+    data = open(path, "rb").read()
+    pos = data.index(b"\n\n") + 2
+    end = data.index(b"\n", pos)
+    parts = data[pos:end].split()
+    if len(parts) != 4 or parts[0] != b"-Y" or parts[2] != b"+X":
+        raise ValueError("Unsupported or corrupt texture image")
+    height, width = int(parts[1]), int(parts[3])
+    pos = end + 1
+    rgbe = np.zeros((height, width, 4), np.uint8)
+    for y in range(height):
+        if width >= 8 and width < 32768 and data[pos] == 2 and data[pos + 1] == 2 and not data[pos + 2] & 0x80:
+            pos += 4
+            for c in range(4):
+                x = 0
+                while x < width:
+                    count = data[pos]
+                    pos += 1
+                    if count > 128:
+                        rgbe[y, x:x + count - 128, c] = data[pos]
+                        pos += 1
+                        x += count - 128
+                    else:
+                        rgbe[y, x:x + count, c] = np.frombuffer(data[pos:pos + count], np.uint8)
+                        pos += count
+                        x += count
+        else:
+            rgbe[y] = np.frombuffer(data[pos:pos + 4 * width], np.uint8).reshape(width, 4)
+            pos += 4 * width
+    exponent = rgbe[..., 3].astype(np.int32)
+    scale = np.where(exponent > 0, np.ldexp(np.float32(1), exponent - 136), 0).astype(F32)
+    return (rgbe[..., :3].astype(F32) * scale[..., None]).astype(F32)
+
+
+def read_texture(path: str, linear: bool) -> np.ndarray:
+    """Image::read (src/core/raster_io.cpp:40-113): (height, width, 3) float32 linear RGB. EXR and
+    HDR files must be declared linear; 8- and 16-bit images are converted from sRGB unless
+    declared linear."""
+    extension = path.lower().rsplit(".", 1)[-1]
+    if extension in ("exr", "hdr"):
+        if not linear:
+            raise ValueError(f"{extension.upper()} textures require linear encoding")
+        image = read_exr(path) if extension == "exr" else read_hdr(path)
+    else:
+        image = read_png(path)
+        if not linear:
+            image = srgb_to_linear(image)
+    if not np.all(np.isfinite(image)):
+        raise ValueError("Texture contains nonfinite samples")
+    return image

@@ -95,7 +95,8 @@ class Transform:
 
 @dataclass
 class Material:
-    """Material (include/minirender/scene/scene.hpp:113-136)."""
+    """Material (include/minirender/scene/scene.hpp:113-136). Textures are indices into
+    SceneDocument.textures (None: no texture)."""
 
     kind: str = "diffuse"
     base_color: tuple = (0.7, 0.7, 0.7)
@@ -103,6 +104,21 @@ class Material:
     roughness: float = 0.35
     ior: float = 1.5
     double_sided: bool = True
+    base_color_texture: int | None = None
+    texture_filter: str = "trilinear"
+    normal_texture: int | None = None
+    normal_scale: float = 1.0
+    normal_flip_y: bool = False
+
+
+@dataclass
+class TextureData:
+    """A decoded texture: (height, width, 3) float32 linear RGB, row 0 at the top
+    (TextureAsset's data, include/minirender/scene/scene.hpp:148-154). `linear` records the source
+    encoding (normal maps must come from linear textures)."""
+
+    rgb: np.ndarray
+    linear: bool = True
 
 
 @dataclass
@@ -196,6 +212,10 @@ class SceneDocument:
     objects: list = field(default_factory=list)
     directional_lights: list = field(default_factory=list)
     media: list = field(default_factory=list)
+    textures: list = field(default_factory=list)  # TextureData
+    environment_texture: int | None = None        # EnvironmentMap (scene.hpp:178-183)
+    environment_strength: float = 1.0
+    environment_rotation_degrees: float = 0.0
 
     @property
     def triangle_count(self) -> int:
@@ -231,12 +251,33 @@ class Snapshot:
         desc.meshes = meshes
         desc.mesh_count = len(document.meshes)
 
+        def one_based(index):
+            return 0 if index is None else int(index) + 1
+
         materials = (_abi.Material * max(1, len(document.materials)))()
         for i, m in enumerate(document.materials):
             materials[i] = _abi.Material(_abi.MATERIAL_KINDS[m.kind], _abi.f3(*m.base_color),
                                          _abi.f3(*m.emission), m.roughness, m.ior,
-                                         1 if m.double_sided else 0)
+                                         1 if m.double_sided else 0,
+                                         one_based(m.base_color_texture),
+                                         _abi.TEXTURE_FILTERS[m.texture_filter],
+                                         one_based(m.normal_texture), m.normal_scale,
+                                         1 if m.normal_flip_y else 0)
         desc.materials = materials
+
+        textures = (_abi.Texture * max(1, len(document.textures)))()
+        for i, t in enumerate(document.textures):
+            rgb = np.ascontiguousarray(t.rgb, dtype=F32)
+            if rgb.ndim != 3 or rgb.shape[2] != 3:
+                raise ValueError("Texture data must be (height, width, 3)")
+            self._keep.append(rgb)
+            textures[i] = _abi.Texture(rgb.ctypes.data_as(C.POINTER(C.c_float)), rgb.shape[1],
+                                       rgb.shape[0])
+        desc.textures = textures
+        desc.texture_count = len(document.textures)
+        desc.environment_texture = one_based(document.environment_texture)
+        desc.environment_strength = document.environment_strength
+        desc.environment_rotation_degrees = document.environment_rotation_degrees
         desc.material_count = len(document.materials)
 
         visible = [o for o in document.objects if o.visible]
@@ -267,7 +308,7 @@ class Snapshot:
                                          r.anisotropy, 1 if r.enabled else 0)
         desc.media = media
         desc.medium_count = len(document.media)
-        self._keep += [meshes, materials, instances, lights, media]
+        self._keep += [meshes, materials, instances, lights, media, textures]
         self.desc = desc
         self.triangle_count = sum(document.meshes[o.mesh].triangle_count for o in visible)
 

@@ -16,9 +16,13 @@ shorter diagonal (corners 0-2 when strictly shorter than 1-3: triangles 0,1,2 an
 matches tinyobjloader for convex polygons. Groups, objects, smoothing and material libraries carry
 no geometry and are ignored.
 
-Not supported by this path tracer (rejected with ValueError naming the feature): environment
-maps, base-colour and normal textures. Cloth and subsurface materials load and are rejected when
-the scene is created, as the C ABI documents.
+Textures (src/assets/scene_io.cpp:111-124): the "textures" table's images are decoded by
+``image_io.read_texture`` (PNG at any bit depth, EXR, Radiance HDR) with their "encoding" ("srgb"
+converts 8/16-bit samples to linear; EXR and HDR must be "linear"); materials reference them by id
+("base_color_texture", "normal_texture" with "normal_scale" and "normal_flip_y", "texture_filter")
+and so does "environment_map" ("texture", "strength", "rotation_degrees"). A normal map must be a
+linear texture (src/scene/scene.cpp:295-301). Cloth and subsurface materials load and are rejected
+when the scene is created, as the C ABI documents.
 """
 
 from __future__ import annotations
@@ -28,8 +32,9 @@ import os
 
 import numpy as np
 
+from .image_io import read_texture, write_exr
 from .scene import (Camera, DirectionalLight, Material, MediumRegion, MeshData, SceneDocument,
-                    SceneObject, Transform)
+                    SceneObject, TextureData, Transform)
 
 F32 = np.float32
 MATERIAL_KINDS = ("diffuse", "conductor", "mirror", "dielectric", "cloth", "subsurface")
@@ -159,22 +164,50 @@ def load_scene(path: str) -> SceneDocument:
                                       _double3(m["absorption"]), _double3(m["scattering"]),
                                       float(m["anisotropy"]), bool(m.get("enabled", True)))
                          for m in media]
-        if data.get("environment_map", {}).get("texture"):
-            raise ValueError("Environment maps are not supported by this path tracer")
+        texture_index = {}
+        for t in data.get("textures", []):
+            encoding = t.get("encoding", "srgb")
+            if encoding not in ("srgb", "linear"):
+                raise ValueError("Unknown texture encoding")
+            if t["id"] in texture_index:
+                raise ValueError(f"Duplicate texture id '{t['id']}'")
+            texture_index[t["id"]] = len(doc.textures)
+            doc.textures.append(TextureData(read_texture(os.path.join(directory, t["source"]),
+                                                         encoding == "linear"),
+                                            encoding == "linear"))
+
+        def texture(name, what):
+            if not name:
+                return None
+            if name not in texture_index:
+                raise ValueError(f"{what} references missing texture: {name}")
+            return texture_index[name]
+
+        environment = data.get("environment_map", {})
+        doc.environment_texture = texture(environment.get("texture", ""), "Environment")
+        doc.environment_strength = float(F32(environment.get("strength", 1.0)))
+        doc.environment_rotation_degrees = float(F32(environment.get("rotation_degrees", 0.0)))
         material_index = {}
         for m in data["materials"]:
             kind = m["kind"]
             if kind not in MATERIAL_KINDS:
                 raise ValueError(f"Unknown material kind '{kind}'")
-            if m.get("base_color_texture") or m.get("normal_texture"):
-                raise ValueError(f"Material '{m['id']}': textures are not supported by this "
-                                 "path tracer")
+            texture_filter = m.get("texture_filter", "trilinear")
+            if texture_filter not in ("nearest", "bilinear", "trilinear"):
+                raise ValueError(f"Unknown texture filter: {texture_filter}")
+            normal = texture(m.get("normal_texture", ""), "Material")
+            if normal is not None and not doc.textures[normal].linear:
+                raise ValueError("Normal map must reference a linear texture")
             material_index[m["id"]] = len(doc.materials)
             doc.materials.append(Material(kind, _vector3(m["base_color"]),
                                           _vector3(m.get("emission", [0, 0, 0])),
                                           float(F32(m.get("roughness", 0.35))),
                                           float(F32(m.get("ior", 1.5))),
-                                          bool(m.get("double_sided", True))))
+                                          bool(m.get("double_sided", True)),
+                                          texture(m.get("base_color_texture", ""), "Material"),
+                                          texture_filter, normal,
+                                          float(F32(m.get("normal_scale", 1.0))),
+                                          bool(m.get("normal_flip_y", False))))
         mesh_index = {}
         for m in data["meshes"]:
             mesh_index[m["id"]] = len(doc.meshes)
@@ -221,6 +254,18 @@ def save_obj(mesh: MeshData, path: str):
         f.write("\n".join(lines) + "\n")
 
 
+def _material_json(k: int, m: Material) -> dict:
+    out = {"id": f"material_{k}", "kind": m.kind, "base_color": list(m.base_color),
+           "emission": list(m.emission), "roughness": m.roughness, "ior": m.ior,
+           "double_sided": bool(m.double_sided), "texture_filter": m.texture_filter,
+           "normal_scale": m.normal_scale, "normal_flip_y": bool(m.normal_flip_y)}
+    if m.base_color_texture is not None:
+        out["base_color_texture"] = f"texture_{m.base_color_texture}"
+    if m.normal_texture is not None:
+        out["normal_texture"] = f"texture_{m.normal_texture}"
+    return out
+
+
 def save_scene(doc: SceneDocument, path: str):
     """Writes a SceneDocument as scene JSON v1 with one OBJ file per mesh beside it
     (mesh_<k>.obj); load_scene reads it back."""
@@ -239,10 +284,7 @@ def save_scene(doc: SceneDocument, path: str):
                    "far": c.far_plane, "aperture_radius": c.aperture_radius,
                    "focus_distance": c.focus_distance},
         "environment": list(doc.environment),
-        "materials": [{"id": f"material_{k}", "kind": m.kind, "base_color": list(m.base_color),
-                       "emission": list(m.emission), "roughness": m.roughness, "ior": m.ior,
-                       "double_sided": bool(m.double_sided)}
-                      for k, m in enumerate(doc.materials)],
+        "materials": [_material_json(k, m) for k, m in enumerate(doc.materials)],
         "meshes": meshes,
         "objects": [{"id": f"object_{k}", "mesh": f"mesh_{o.mesh}",
                      "material": f"material_{o.material}", "visible": bool(o.visible),
@@ -254,6 +296,16 @@ def save_scene(doc: SceneDocument, path: str):
                                 "color": list(l.color), "intensity": l.intensity}
                                for k, l in enumerate(doc.directional_lights)],
     }
+    if doc.textures:
+        data["textures"] = []
+        for k, t in enumerate(doc.textures):
+            name = f"{stem}_texture_{k}.exr"  # linear float: the decoded texels round-trip exactly
+            write_exr(os.path.join(directory, name), t.rgb)
+            data["textures"].append({"id": f"texture_{k}", "source": name, "encoding": "linear"})
+    if doc.environment_texture is not None:
+        data["environment_map"] = {"texture": f"texture_{doc.environment_texture}",
+                                   "strength": doc.environment_strength,
+                                   "rotation_degrees": doc.environment_rotation_degrees}
     if doc.media:
         data["media"] = [{"id": f"medium_{k}", "minimum": list(m.minimum),
                           "maximum": list(m.maximum), "absorption": list(m.absorption),

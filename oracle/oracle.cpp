@@ -396,6 +396,124 @@ class RayQuery {  // intersection.cpp:52-152
     double shear_x_ = 0, shear_y_ = 0, scale_z_ = 1;
 };
 
+// ---- textures (src/core/texture.cpp) -------------------------------------------------------
+
+struct fvec2 {
+    float x = 0, y = 0;
+};
+
+struct Image {  // linear RGB, origin top-left
+    std::size_t        width = 0, height = 0;
+    std::vector<fvec3> pixels;
+    const fvec3& at(std::size_t x, std::size_t y) const { return pixels[y * width + x]; }
+};
+
+int wrap(int coordinate, int extent) {  // texture.cpp:13-15
+    return (coordinate % extent + extent) % extent;
+}
+
+fvec2 image_uv(fvec2 uv) {  // texture.cpp:17-22
+    if (!std::isfinite(uv.x) || !std::isfinite(uv.y)) {
+        throw std::invalid_argument("Texture coordinates must be finite");
+    }
+    return {uv.x - std::floor(uv.x), 1.0F - (uv.y - std::floor(uv.y))};
+}
+
+// glm::mix of float vectors: x * (1 - a) + y * a.
+fvec3 mixf(fvec3 x, fvec3 y, float a) {
+    const float b = 1.0F - a;
+    return {x.x * b + y.x * a, x.y * b + y.y * a, x.z * b + y.z * a};
+}
+
+Image downsample(const Image& source) {  // texture.cpp:25-50
+    Image target;
+    target.width  = std::max(std::size_t(1), source.width / 2);
+    target.height = std::max(std::size_t(1), source.height / 2);
+    target.pixels.resize(target.width * target.height);
+    for (std::size_t y = 0; y < target.height; ++y) {
+        for (std::size_t x = 0; x < target.width; ++x) {
+            const double left   = double(x) * double(source.width) / double(target.width);
+            const double right  = double(x + 1) * double(source.width) / double(target.width);
+            const double top    = double(y) * double(source.height) / double(target.height);
+            const double bottom = double(y + 1) * double(source.height) / double(target.height);
+            dvec3        sum;
+            double       weight_sum = 0;
+            for (std::size_t sy = static_cast<std::size_t>(top); sy < static_cast<std::size_t>(std::ceil(bottom));
+                 ++sy) {
+                for (std::size_t sx = static_cast<std::size_t>(left);
+                     sx < static_cast<std::size_t>(std::ceil(right)); ++sx) {
+                    const double weight = (std::min(right, double(sx + 1)) - std::max(left, double(sx))) *
+                                          (std::min(bottom, double(sy + 1)) - std::max(top, double(sy)));
+                    sum += widen(source.at(sx, sy)) * weight;
+                    weight_sum += weight;
+                }
+            }
+            target.pixels[y * target.width + x] = narrow(sum / weight_sum);
+        }
+    }
+    return target;
+}
+
+class Texture {  // texture.cpp:54-139
+  public:
+    explicit Texture(Image image) {
+        if (image.width > 16384 || image.height > 16384 || image.width * image.height > 64u * 1024u * 1024u) {
+            throw std::invalid_argument("Texture exceeds the 64-megapixel budget");
+        }
+        for (const auto& p : image.pixels) {
+            if (!finite3(p)) {
+                throw std::invalid_argument("Texture contains nonfinite samples");
+            }
+        }
+        levels_.push_back(std::move(image));
+        while (levels_.back().width > 1 || levels_.back().height > 1) {
+            levels_.push_back(downsample(levels_.back()));
+        }
+    }
+    const Image& level(std::size_t index) const { return levels_.at(index); }
+    std::size_t  level_count() const noexcept { return levels_.size(); }
+
+    fvec3 sample(fvec2 uv, float lod, std::uint32_t filter) const {
+        if (!std::isfinite(lod)) {
+            throw std::invalid_argument("Texture LOD must be finite");
+        }
+        if (filter == MR_FILTER_NEAREST) {
+            const auto   coordinate = image_uv(uv);
+            const auto&  image      = levels_.front();
+            const int    x          = static_cast<int>(std::floor(coordinate.x * static_cast<float>(image.width)));
+            const int    y          = static_cast<int>(std::floor(coordinate.y * static_cast<float>(image.height)));
+            return image.at(static_cast<std::size_t>(wrap(x, static_cast<int>(image.width))),
+                            static_cast<std::size_t>(wrap(y, static_cast<int>(image.height))));
+        }
+        if (filter == MR_FILTER_BILINEAR) {
+            return bilinear(uv, 0);
+        }
+        const float clamped = std::clamp(lod, 0.0F, static_cast<float>(levels_.size() - 1));
+        const auto  lower   = static_cast<std::size_t>(std::floor(clamped));
+        const auto  upper   = std::min(lower + 1, levels_.size() - 1);
+        return mixf(bilinear(uv, lower), bilinear(uv, upper), clamped - static_cast<float>(lower));
+    }
+
+  private:
+    fvec3 bilinear(fvec2 uv, std::size_t level_index) const {
+        const auto& image      = levels_.at(level_index);
+        const auto  coordinate = image_uv(uv);
+        const float x          = coordinate.x * static_cast<float>(image.width) - 0.5F;
+        const float y          = coordinate.y * static_cast<float>(image.height) - 0.5F;
+        const int   ix         = static_cast<int>(std::floor(x));
+        const int   iy         = static_cast<int>(std::floor(y));
+        const float tx         = x - std::floor(x);
+        const float ty         = y - std::floor(y);
+        const auto  texel      = [&](int px, int py) {
+            return image.at(static_cast<std::size_t>(wrap(px, static_cast<int>(image.width))),
+                            static_cast<std::size_t>(wrap(py, static_cast<int>(image.height))));
+        };
+        return mixf(mixf(texel(ix, iy), texel(ix + 1, iy), tx), mixf(texel(ix, iy + 1), texel(ix + 1, iy + 1), tx),
+                    ty);
+    }
+    std::vector<Image> levels_;
+};
+
 // ---- scene snapshot ---------------------------------------------------------------------
 
 struct Material {
@@ -405,11 +523,17 @@ struct Material {
     float         roughness    = 0.35F;
     float         ior          = 1.5F;
     bool          double_sided = true;
+    std::uint32_t texture_filter = MR_FILTER_TRILINEAR;
+    float         normal_scale   = 1;
+    bool          normal_flip_y  = false;
+    // RenderInstance's resolved textures (include/minirender/scene/scene.hpp:201-209).
+    std::shared_ptr<const Texture> base_color_texture, normal_texture;
 };
 
 struct Corner {
     std::uint32_t position;
     fvec3         normal;
+    fvec2         uv;
 };
 
 struct Mesh {
@@ -443,6 +567,9 @@ struct Snapshot {
     std::vector<Instance>             instances;
     std::vector<DirectionalLightDesc> directional_lights;
     std::vector<MediumRegion>         media;
+    std::shared_ptr<const Texture>    environment_texture;
+    float                             environment_strength         = 1;
+    float                             environment_rotation_degrees = 0;
 };
 
 // glm::vec3(object_to_world * glm::vec4(p, 1)) in float (bvh.cpp:68-69).
@@ -506,6 +633,29 @@ std::shared_ptr<Snapshot> make_snapshot(const mr_scene_desc& d) {
     require(finite3(s->environment) && s->environment.x >= 0 && s->environment.y >= 0 &&
                 s->environment.z >= 0,
             "Environment must be finite and nonnegative");
+    std::vector<std::shared_ptr<const Texture>> textures;
+    for (std::uint32_t i = 0; i < d.texture_count; ++i) {
+        const auto& src = d.textures[i];
+        require(src.width > 0 && src.height > 0 && src.rgb, "Texture data is missing");
+        Image image;
+        image.width  = src.width;
+        image.height = src.height;
+        image.pixels.resize(static_cast<std::size_t>(src.width) * src.height);
+        for (std::size_t k = 0; k < image.pixels.size(); ++k) {
+            image.pixels[k] = {src.rgb[3 * k], src.rgb[3 * k + 1], src.rgb[3 * k + 2]};
+        }
+        textures.push_back(std::make_shared<const Texture>(std::move(image)));
+    }
+    const auto texture = [&](std::uint32_t one_based) -> std::shared_ptr<const Texture> {
+        if (one_based == 0) {
+            return nullptr;
+        }
+        require(one_based <= textures.size(), "Material references missing texture");
+        return textures[one_based - 1];
+    };
+    s->environment_texture          = texture(d.environment_texture);
+    s->environment_strength         = d.environment_strength;
+    s->environment_rotation_degrees = d.environment_rotation_degrees;
     std::vector<std::shared_ptr<const Mesh>> meshes;
     for (std::uint32_t i = 0; i < d.mesh_count; ++i) {
         const auto& src = d.meshes[i];
@@ -523,8 +673,9 @@ std::shared_ptr<Snapshot> make_snapshot(const mr_scene_desc& d) {
             for (int c = 0; c < 3; ++c) {
                 const auto& corner = src.corners[3 * t + c];
                 require(corner.position < src.position_count, "Mesh position index is out of range");
-                m->triangles[t][c] = {corner.position, fvec3{corner.normal[0], corner.normal[1],
-                                                             corner.normal[2]}};
+                m->triangles[t][c] = {corner.position,
+                                      fvec3{corner.normal[0], corner.normal[1], corner.normal[2]},
+                                      fvec2{corner.uv[0], corner.uv[1]}};
             }
         }
         meshes.push_back(m);
@@ -539,6 +690,13 @@ std::shared_ptr<Snapshot> make_snapshot(const mr_scene_desc& d) {
         m.roughness    = src.roughness;
         m.ior          = src.ior;
         m.double_sided = src.double_sided != 0;
+        m.texture_filter     = src.texture_filter;
+        m.normal_scale       = src.normal_scale;
+        m.normal_flip_y      = src.normal_flip_y != 0;
+        m.base_color_texture = texture(src.base_color_texture);
+        m.normal_texture     = texture(src.normal_texture);
+        require(m.texture_filter <= MR_FILTER_TRILINEAR, "Unknown texture filter");
+        require(std::isfinite(m.normal_scale), "Normal scale must be finite");
         require(finite3(m.base_color) && m.base_color.x >= 0 && m.base_color.y >= 0 &&
                     m.base_color.z >= 0 && m.base_color.x <= 1 && m.base_color.y <= 1 &&
                     m.base_color.z <= 1,
@@ -611,6 +769,7 @@ struct SurfaceHit {
     dvec3         position;
     fvec3         geometric_normal;
     fvec3         shading_normal;
+    fvec2         uv;
     dvec3         barycentric;
     std::uint32_t instance_index = 0;
     std::uint32_t triangle_index = 0;
@@ -618,6 +777,35 @@ struct SurfaceHit {
     bool          front_face     = true;
     dvec3         position_error;
 };
+
+// uv_tangents (src/geometry/uv_tangents.cpp:12-36): the triangle's unit dP/du and dP/dv.
+bool uv_tangents(const std::array<fvec3, 3>& positions, const std::array<fvec2, 3>& coordinates, dvec3& u_axis,
+                 dvec3& v_axis) {
+    const auto a = widen(positions[1]) - widen(positions[0]);
+    const auto b = widen(positions[2]) - widen(positions[0]);
+    dvec2 s{double(coordinates[1].x) - double(coordinates[0].x), double(coordinates[1].y) - double(coordinates[0].y)};
+    dvec2 t{double(coordinates[2].x) - double(coordinates[0].x), double(coordinates[2].y) - double(coordinates[0].y)};
+    const double scale = std::max({std::abs(s.x), std::abs(s.y), std::abs(t.x), std::abs(t.y)});
+    if (!std::isfinite(scale) || scale == 0) {
+        return false;
+    }
+    s.x /= scale, s.y /= scale;
+    t.x /= scale, t.y /= scale;
+    const double determinant = s.x * t.y - s.y * t.x;
+    if (!std::isfinite(determinant) || std::abs(determinant) < 1e-12) {
+        return false;
+    }
+    const auto   u  = (t.y * a - s.y * b) / determinant;
+    const auto   v  = (-t.x * a + s.x * b) / determinant;
+    const double lu = length(u);
+    const double lv = length(v);
+    if (!std::isfinite(lu) || !std::isfinite(lv) || lu == 0 || lv == 0) {
+        return false;
+    }
+    u_axis = u / lu;
+    v_axis = v / lv;
+    return true;
+}
 
 struct BvhStatistics {
     std::size_t triangles = 0, nodes = 0, leaves = 0, maximum_depth = 0;
@@ -890,7 +1078,7 @@ class SceneBvh {
         return result;
     }
 
-    // bvh.cpp:302-370 without normal maps (the configs have none).
+    // bvh.cpp:302-370, normal maps decoded in the triangle's UV tangent frame.
     SurfaceHit surface_hit(const Ray& ray, const PrimitiveHit& hit) const {
         const auto& primitive = primitives_[hit.primitive];
         const auto& instance  = scene_->instances[primitive.instance];
@@ -901,11 +1089,14 @@ class SceneBvh {
         if (mirrored_[primitive.instance]) {
             geometric = -geometric;
         }
-        dvec3 shading, position, absolute_position;
+        dvec3  shading, position, absolute_position;
+        dvec2  uv;
         for (int corner = 0; corner < 3; ++corner) {
             const double weight = hit.hit.barycentric[corner];
             shading += weight * normalize(transform_normal(instance.normal_to_world,
                                                            triangle[corner].normal));
+            uv.x += weight * static_cast<double>(triangle[corner].uv.x);
+            uv.y += weight * static_cast<double>(triangle[corner].uv.y);
             const auto term = weight * widen(primitive.vertices[corner]);
             position += term;
             absolute_position += dabs(term);
@@ -918,11 +1109,37 @@ class SceneBvh {
                 shading = -shading;
             }
         }
+        const fvec2 uv_f{static_cast<float>(uv.x), static_cast<float>(uv.y)};
+        const auto& material = instance.material;
+        if (material.normal_texture && material.normal_scale > 0) {
+            const std::array<fvec2, 3> coords{triangle[0].uv, triangle[1].uv, triangle[2].uv};
+            dvec3 axis_u, axis_v;
+            if (uv_tangents(primitive.vertices, coords, axis_u, axis_v)) {
+                const auto t0 = axis_u - shading * dot(axis_u, shading);
+                if (dot(t0, t0) > 1e-12) {
+                    const auto t = normalize(t0);
+                    auto       b = cross(shading, t);
+                    if (dot(b, axis_v) < 0) {
+                        b = -b;
+                    }
+                    // glm::dvec3(sample) * 2. - 1.
+                    auto sample = widen(material.normal_texture->sample(uv_f, 0, material.texture_filter)) * 2.0 -
+                                  dvec3{1, 1, 1};
+                    sample.x *= material.normal_scale;
+                    sample.y *= material.normal_scale * (material.normal_flip_y ? -1. : 1.);
+                    const auto mapped = t * sample.x + b * sample.y + shading * sample.z;
+                    if (dot(mapped, geometric) > 1e-8) {
+                        shading = normalize(mapped);
+                    }
+                }
+            }
+        }
         SurfaceHit result;
         result.distance         = hit.hit.distance;
         result.position         = position;
         result.geometric_normal = narrow(geometric);
         result.shading_normal   = narrow(shading);
+        result.uv               = uv_f;
         result.barycentric      = hit.hit.barycentric;
         result.instance_index   = primitive.instance;
         result.triangle_index   = primitive.triangle;
@@ -1078,8 +1295,13 @@ struct BsdfSample {
 
 class Bsdf {  // bsdf.cpp:122-277 without cloth and energy compensation
   public:
-    Bsdf(const Material& material, bool front_face, bool importance = false)
-        : kind_(material.kind), color_(widen(material.base_color)),
+    // color = base_color * clamp(texture colour, 0, 1) (bsdf.cpp:122-141).
+    Bsdf(const Material& material, bool front_face, bool importance = false,
+         fvec3 texture_color = fvec3{1, 1, 1})
+        : kind_(material.kind),
+          color_(widen(material.base_color) * dvec3{std::clamp(double(texture_color.x), 0.0, 1.0),
+                                                    std::clamp(double(texture_color.y), 0.0, 1.0),
+                                                    std::clamp(double(texture_color.z), 0.0, 1.0)}),
           alpha_(static_cast<double>(material.roughness) * material.roughness),
           eta_i_(front_face ? 1 : material.ior), eta_t_(front_face ? material.ior : 1),
           importance_(importance) {}
@@ -1181,6 +1403,156 @@ double area_density(dvec3 reference, dvec3 point, dvec3 normal, double area) {  
     return cosine > 0 ? squared_distance / (area * cosine) : 0;
 }
 
+dvec3 positive(dvec3 c) { return {std::max(c.x, 0.0), std::max(c.y, 0.0), std::max(c.z, 0.0)}; }  // light.cpp:25-27
+
+dvec3 unit_light_direction(dvec3 direction) {  // light.cpp:35-40
+    if (!finite3(direction) || std::abs(dot(direction, direction) - 1) > 1e-4) {
+        throw std::invalid_argument("Light direction must be finite and have unit length");
+    }
+    return normalize(direction);
+}
+
+// glm::mix of double vectors: x * (1 - a) + y * a.
+dvec3 mixd(dvec3 x, dvec3 y, double a) { return x * (1 - a) + y * a; }
+
+constexpr double uniform_fraction = 0.05;  // light.cpp:15
+
+// EnvironmentLight (light.cpp:61-195): constant radiance plus an optional lat-long map (origin at
+// the image's top left, +Y north, longitude 0 along +X increasing towards +Z), importance-sampled
+// over a grid of at most 1024x512 texels (a mip level) weighted by luminance and solid angle,
+// mixed with 5% uniform sphere density.
+class EnvironmentLight {
+  public:
+    explicit EnvironmentLight(const Snapshot& scene)
+        : constant_(widen(scene.environment)), texture_(scene.environment_texture),
+          strength_(scene.environment_strength),
+          rotation_(std::remainder(static_cast<double>(scene.environment_rotation_degrees), 360.0) * pi / 180),
+          integral_(4 * pi * luminance(constant_)) {
+        if (!texture_ || strength_ == 0) {
+            return;
+        }
+        while (texture_->level(grid_level_).width > 1024 || texture_->level(grid_level_).height > 512) {
+            ++grid_level_;
+        }
+        const auto&         image = texture_->level(grid_level_);
+        std::vector<double> weights;
+        weights.reserve(image.width * image.height);
+        double map_integral = 0;
+        for (std::size_t y = 0; y < image.height; ++y) {
+            const double theta0 = pi * static_cast<double>(y) / static_cast<double>(image.height);
+            const double theta1 = pi * static_cast<double>(y + 1) / static_cast<double>(image.height);
+            const double angle  = (2 * pi / static_cast<double>(image.width)) * 2 *
+                                 std::sin((theta0 + theta1) * 0.5) * std::sin((theta1 - theta0) * 0.5);
+            solid_angles_.push_back(angle);
+            for (std::size_t x = 0; x < image.width; ++x) {
+                const double weight = luminance(positive(widen(image.at(x, y)))) * angle;
+                weights.push_back(weight);
+                map_integral += weight;
+            }
+        }
+        pixels_  = DiscreteDistribution(weights);
+        uniform_ = map_integral == 0;
+        double      full_integral = 0;
+        const auto& full          = texture_->level(0);
+        for (std::size_t y = 0; y < full.height; ++y) {
+            const double theta0 = pi * static_cast<double>(y) / static_cast<double>(full.height);
+            const double theta1 = pi * static_cast<double>(y + 1) / static_cast<double>(full.height);
+            const double angle  = (2 * pi / static_cast<double>(full.width)) * 2 *
+                                 std::sin((theta0 + theta1) * 0.5) * std::sin((theta1 - theta0) * 0.5);
+            for (std::size_t x = 0; x < full.width; ++x) {
+                full_integral += luminance(positive(widen(full.at(x, y)))) * angle;
+            }
+        }
+        integral_ += strength_ * full_integral;
+    }
+
+    dvec2 coordinates(dvec3 direction) const {  // light.cpp:112-119
+        direction = unit_light_direction(direction);
+        double u  = (std::atan2(direction.z, direction.x) + rotation_) / (2 * pi);
+        u -= std::floor(u);
+        const double v = std::atan2(std::hypot(direction.x, direction.z), direction.y) / pi;
+        return {u, v};
+    }
+
+    dvec3 lookup(dvec2 uv) const {  // light.cpp:121-138
+        const auto&  image = texture_->level(0);
+        const double x     = uv.x * static_cast<double>(image.width) - 0.5;
+        const double y     = uv.y * static_cast<double>(image.height) - 0.5;
+        const int    ix    = static_cast<int>(std::floor(x));
+        const int    iy    = static_cast<int>(std::floor(y));
+        const double tx    = x - std::floor(x);
+        const double ty    = y - std::floor(y);
+        const auto   texel = [&](int column, int row) {
+            const int width = static_cast<int>(image.width), height = static_cast<int>(image.height);
+            const auto wrapped = static_cast<std::size_t>((column % width + width) % width);
+            return positive(widen(image.at(wrapped, static_cast<std::size_t>(std::clamp(row, 0, height - 1)))));
+        };
+        return mixd(mixd(texel(ix, iy), texel(ix + 1, iy), tx), mixd(texel(ix, iy + 1), texel(ix + 1, iy + 1), tx),
+                    ty);
+    }
+
+    dvec3 evaluate(dvec3 direction) const {  // light.cpp:140-143
+        const auto uv = coordinates(direction);
+        return constant_ + (texture_ ? strength_ * lookup(uv) : dvec3{0, 0, 0});
+    }
+
+    double pdf(dvec3 direction) const {  // light.cpp:145-157
+        const auto uv = coordinates(direction);
+        if (uniform_) {
+            return 1 / (4 * pi);
+        }
+        const auto& grid = texture_->level(grid_level_);
+        const auto  x    = std::min(static_cast<std::size_t>(uv.x * static_cast<double>(grid.width)), grid.width - 1);
+        const auto  y    = std::min(static_cast<std::size_t>(uv.y * static_cast<double>(grid.height)), grid.height - 1);
+        return uniform_fraction / (4 * pi) +
+               (1 - uniform_fraction) * pixels_.probability(y * grid.width + x) / solid_angles_[y];
+    }
+
+    // light.cpp:159-191: direction, radiance, density.
+    void sample(dvec2 u, dvec3& direction, dvec3& radiance, double& density) const {
+        check_unit(u);
+        if (uniform_ || u.x < uniform_fraction) {
+            direction = sample_sphere({uniform_ ? u.x : u.x / uniform_fraction, u.y});
+        } else {
+            const auto   selected = pixels_.sample((u.x - uniform_fraction) / (1 - uniform_fraction));
+            const auto&  grid     = texture_->level(grid_level_);
+            const auto   x = selected->index % grid.width, y = selected->index / grid.width;
+            const double theta0 = pi * static_cast<double>(y) / static_cast<double>(grid.height);
+            const double theta1 = pi * static_cast<double>(y + 1) / static_cast<double>(grid.height);
+            const double difference = 2 * std::sin((theta0 + theta1) * 0.5) * std::sin((theta1 - theta0) * 0.5);
+            const double v = std::clamp(u.y, dbl_eps * 0.5, std::nextafter(1.0, 0.0));
+            double       cosine, sine;
+            if (y < grid.height / 2) {
+                const double h = 1 - std::cos(theta0) + v * difference;
+                cosine         = 1 - h;
+                sine           = std::sqrt(std::max(0.0, h * (2 - h)));
+            } else {
+                const double h = 1 + std::cos(theta1) + (1 - v) * difference;
+                cosine         = -1 + h;
+                sine           = std::sqrt(std::max(0.0, h * (2 - h)));
+            }
+            const double phi = 2 * pi * (static_cast<double>(x) + selected->remapped) / static_cast<double>(grid.width) -
+                               rotation_;
+            direction = {sine * std::cos(phi), cosine, sine * std::sin(phi)};
+        }
+        radiance = evaluate(direction);
+        density  = pdf(direction);
+    }
+
+    double luminance_integral() const noexcept { return integral_; }
+
+  private:
+    dvec3                          constant_;
+    std::shared_ptr<const Texture> texture_;
+    double                         strength_ = 1;
+    double                         rotation_ = 0;
+    double                         integral_ = 0;
+    bool                           uniform_  = true;
+    std::size_t                    grid_level_ = 0;
+    std::vector<double>            solid_angles_;
+    DiscreteDistribution           pixels_;
+};
+
 enum class LightKind { area, directional, environment };
 
 struct LightSample {
@@ -1194,10 +1566,10 @@ struct LightSample {
     dvec3       position, normal, position_error;
 };
 
-class LightSampler {  // light.cpp:61-354, constant environment only
+class LightSampler {  // light.cpp:197-352
   public:
-    explicit LightSampler(const Snapshot& scene) : constant_(widen(scene.environment)) {
-        integral_ = 4 * pi * luminance(constant_);  // light.cpp:66
+    explicit LightSampler(const Snapshot& scene) : environment_(scene) {
+        integral_ = environment_.luminance_integral();
         Bounds3             bounds;
         std::vector<double> weights;
         for (std::size_t index = 0; index < scene.instances.size(); ++index) {
@@ -1252,8 +1624,8 @@ class LightSampler {  // light.cpp:61-354, constant environment only
         selection_ = DiscreteDistribution(weights);
     }
 
-    dvec3  environment_evaluate(dvec3) const { return constant_; }           // light.cpp:140-143
-    double environment_density(dvec3) const { return 1 / (4 * pi); }        // light.cpp:145-148
+    dvec3  environment_evaluate(dvec3 direction) const { return environment_.evaluate(direction); }
+    double environment_density(dvec3 direction) const { return environment_.pdf(direction); }
 
     std::optional<LightSample> sample(dvec3 reference, double light_u, dvec2 surface_u) const {
         if (!finite3(reference)) {
@@ -1277,11 +1649,10 @@ class LightSampler {  // light.cpp:61-354, constant environment only
             return s;
         }
         if (choice.kind == LightKind::environment) {
-            const auto  direction = sample_sphere({surface_u.x, surface_u.y});  // light.cpp:162-163
             LightSample s;
-            s.direction   = direction;
-            s.radiance    = environment_evaluate(direction);
-            s.probability = selected->probability * environment_density(direction);
+            double      density = 0;
+            environment_.sample(surface_u, s.direction, s.radiance, density);
+            s.probability = selected->probability * density;
             s.kind        = choice.kind;
             s.emitter     = selected->index;
             return s;
@@ -1352,7 +1723,7 @@ class LightSampler {  // light.cpp:61-354, constant environment only
         LightKind   kind;
         std::size_t index;
     };
-    dvec3                                                           constant_;
+    EnvironmentLight                                                environment_;
     double                                                          integral_ = 0;
     std::vector<Area>                                               areas_;
     std::vector<Directional>                                        directional_;
@@ -1769,7 +2140,11 @@ class PathTracer {
             }
             const ShadingFrame frame(normal);
             const auto         wo = frame.to_local(wo_world);
-            const Bsdf         bsdf(instance.material, hit->front_face);
+            const fvec3 texture_color = instance.material.base_color_texture
+                                            ? instance.material.base_color_texture->sample(
+                                                  hit->uv, 0, instance.material.texture_filter)
+                                            : fvec3{1, 1, 1};  // path_tracer.cpp:279-282
+            const Bsdf         bsdf(instance.material, hit->front_face, false, texture_color);
             const double       light_u     = sampler.next_1d();
             const auto         surface_u   = sampler.next_2d();
             const double       component   = sampler.next_1d();

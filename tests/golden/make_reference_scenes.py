@@ -18,7 +18,7 @@ sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 
 from minirender_b200 import scene_io  # noqa: E402
 
-SCENES = ("studio", "path-room")
+SCENES = ("studio", "path-room", "studio-textured")
 
 
 def main() -> None:
