@@ -483,7 +483,7 @@ void build_instance_tree(Scene& scene, cudaStream_t stream) {
     lo.allocate(count);
     hi.allocate(count);
     centroid.allocate(count);
-    instance_boxes_kernel<<<grid(count), 128, 0, stream>>>(t.instances.ptr, count, d_boxes.ptr, d_mesh.ptr, lo.ptr,
+    instance_boxes_kernel<<<grid(count, 128), 128, 0, stream>>>(t.instances.ptr, count, d_boxes.ptr, d_mesh.ptr, lo.ptr,
                                                            hi.ptr, centroid.ptr);
     MR_CUDA(cudaGetLastError());
     BuildResult built = build_bvh_device(lo.ptr, hi.ptr, centroid.ptr, count, stream);
@@ -604,12 +604,12 @@ void refit_mesh(Scene& scene, uint32_t mesh, const float* device_positions, cuda
         lo.ptr, hi.ptr, centroid.ptr);
     parents_kernel<<<grid(mt.node_count), 256, 0, stream>>>(mt.nodes.ptr, mt.node_count, parent.ptr);
     MR_CUDA(cudaMemsetAsync(arrivals.ptr, 0, mt.node_count * sizeof(uint32_t), stream));
-    refit_kernel<<<grid(mt.node_count), 128, 0, stream>>>(mt.nodes.ptr, mt.node_count, parent.ptr, mt.order.ptr,
+    refit_kernel<<<grid(mt.node_count, 128), 128, 0, stream>>>(mt.nodes.ptr, mt.node_count, parent.ptr, mt.order.ptr,
                                                           lo.ptr, hi.ptr, arrivals.ptr);
     MR_CUDA(cudaGetLastError());
     // Same wide topology: each wide node takes its children's refit boxes.
     if (mt.wide_count) {
-        refit_wide_kernel<<<grid(mt.wide_count), 128, 0, stream>>>(mt.nodes.ptr, mt.wide_children.ptr,
+        refit_wide_kernel<<<grid(mt.wide_count, 128), 128, 0, stream>>>(mt.nodes.ptr, mt.wide_children.ptr,
                                                                    mt.wide_count,
                                                                    t.blas_nodes.ptr + 8ull * mt.node_base);
     }

@@ -45,9 +45,8 @@ constexpr size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
 // Byte size of the carved regions (same fields as a pooled Workspace, plus ray staging and a
 // validation word).
 constexpr size_t kScratchBytes =
-    align256(kStaticPaths * sizeof(ulonglong2)) + 7 * align256(kStaticPaths * sizeof(float4)) +
-    align256(kStaticPaths * sizeof(uint32_t)) + 3 * align256(kStaticPaths * sizeof(float4)) +
-    align256(kStaticPaths * sizeof(uint32_t)) + 2 * align256(kStaticPaths * sizeof(uint32_t)) +
+    align256(kStaticPaths * kPathRecordBytes) + align256(kStaticPaths * kShadowRecordBytes) +
+    2 * align256(kStaticPaths * sizeof(uint32_t)) +
     align256(kStaticPaths * kBinCount * sizeof(uint32_t)) + align256(kStaticPaths * sizeof(uint32_t)) +
     align256((kStaticBounces + 2) * sizeof(BounceCounters)) +
     align256(kStatCount * sizeof(unsigned long long)) + align256(sizeof(unsigned)) +
@@ -84,19 +83,8 @@ void carve(unsigned char* base, Workspace& ws, float4*& staging, unsigned*& inva
     ws.memory            = nullptr;
     ws.pixels            = 0;
     ws.accumulator       = nullptr;
-    ws.state.rng         = reinterpret_cast<ulonglong2*>(take(kStaticPaths * sizeof(ulonglong2)));
-    ws.state.beta        = reinterpret_cast<float4*>(take(kStaticPaths * sizeof(float4)));
-    ws.state.radiance    = reinterpret_cast<float4*>(take(kStaticPaths * sizeof(float4)));
-    ws.state.prev        = reinterpret_cast<float4*>(take(kStaticPaths * sizeof(float4)));
-    ws.state.ray_o       = reinterpret_cast<float4*>(take(kStaticPaths * sizeof(float4)));
-    ws.state.ray_d       = reinterpret_cast<float4*>(take(kStaticPaths * sizeof(float4)));
-    ws.state.hit         = reinterpret_cast<float4*>(take(kStaticPaths * sizeof(float4)));
-    ws.state.shadow_o    = reinterpret_cast<float4*>(take(kStaticPaths * sizeof(float4)));
-    ws.state.flags       = reinterpret_cast<uint32_t*>(take(kStaticPaths * sizeof(uint32_t)));
-    ws.state.shadow_d    = reinterpret_cast<float4*>(take(kStaticPaths * sizeof(float4)));
-    ws.state.shadow_c    = reinterpret_cast<float4*>(take(kStaticPaths * sizeof(float4)));
-    take(kStaticPaths * sizeof(float4));  // spare record keeps the size formula in one shape
-    ws.state.hit_slot    = reinterpret_cast<uint32_t*>(take(kStaticPaths * sizeof(uint32_t)));
+    unsigned char* paths = take(kStaticPaths * kPathRecordBytes);
+    ws.state.view(paths, take(kStaticPaths * kShadowRecordBytes), false);
     ws.queues.ext[0]     = reinterpret_cast<uint32_t*>(take(kStaticPaths * sizeof(uint32_t)));
     ws.queues.ext[1]     = reinterpret_cast<uint32_t*>(take(kStaticPaths * sizeof(uint32_t)));
     ws.queues.bins       = reinterpret_cast<uint32_t*>(take(kStaticPaths * kBinCount * sizeof(uint32_t)));

@@ -638,7 +638,7 @@ __device__ __forceinline__ void neumaier(float& sum, float& comp, float v) {
 
 // Adds the wave's per-path radiance to the pixels in sample order; checks every path result
 // like check_radiance (src/render/path_tracer.cpp:22-26).
-__global__ void resolve_kernel(const float4* radiance, uint32_t x0, uint32_t y0, uint32_t w,
+__global__ void resolve_kernel(PathField<float4> radiance, uint32_t x0, uint32_t y0, uint32_t w,
                                uint32_t h, uint32_t ns, uint32_t width, float4* accumulator,
                                uint32_t accumulator_row0, unsigned* error) {
     const uint32_t r    = blockIdx.x * blockDim.x + threadIdx.x;
@@ -670,7 +670,7 @@ __global__ void resolve_kernel(const float4* radiance, uint32_t x0, uint32_t y0,
 // from zero), and a pixel whose last sample this is gets its mean written to the job's image with
 // the overflow check. Same arithmetic as resolve_kernel + finalize_kernel, so a job's image does
 // not depend on which wave carried which of its samples.
-__global__ void __launch_bounds__(256) resolve_batch_kernel(const float4* radiance, const WaveDesc* w,
+__global__ void __launch_bounds__(256) resolve_batch_kernel(PathField<float4> radiance, const WaveDesc* w,
                                                             unsigned* error) {
     const uint32_t n        = w->pixels;
     const uint32_t segments = w->segments;
@@ -747,7 +747,7 @@ __global__ void capture_shadow_kernel(KernelArgs a, float4* rays, uint8_t* has_s
     }
 }
 
-__global__ void copy_radiance_kernel(const float4* radiance, uint32_t count, float* out) {
+__global__ void copy_radiance_kernel(PathField<float4> radiance, uint32_t count, float* out) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < count) {
         const float4 v = radiance[i];
@@ -816,19 +816,8 @@ std::shared_ptr<Workspace> allocate_workspace(size_t capacity, uint32_t max_boun
         offset += align_up(bytes);
         return at;
     };
-    const size_t o_rng = field(capacity * sizeof(ulonglong2));
-    const size_t o_beta = field(capacity * sizeof(float4));
-    const size_t o_rad = field(capacity * sizeof(float4));
-    const size_t o_prev = field(capacity * sizeof(float4));
-    const size_t o_flags = field(capacity * sizeof(uint32_t));
-    const size_t o_ro = field(capacity * sizeof(float4));
-    const size_t o_rd = field(capacity * sizeof(float4));
-    const size_t o_hit = field(capacity * sizeof(float4));
-    const size_t o_slot = field(capacity * sizeof(uint32_t));
-    const size_t o_so = field(capacity * sizeof(float4));
-    const size_t o_sd = field(capacity * sizeof(float4));
-    const size_t o_sc = field(capacity * sizeof(float4));
-    const size_t o_seg = field(capacity * sizeof(uint32_t));
+    const size_t o_paths   = field(capacity * kPathRecordBytes);
+    const size_t o_shadows = field(capacity * kShadowRecordBytes);
     const size_t o_e0 = field(capacity * sizeof(uint32_t));
     const size_t o_e1 = field(capacity * sizeof(uint32_t));
     const size_t o_bins = field(capacity * kBinCount * sizeof(uint32_t));
@@ -845,19 +834,8 @@ std::shared_ptr<Workspace> allocate_workspace(size_t capacity, uint32_t max_boun
     ws->capacity            = capacity;
     ws->max_bounces         = max_bounces;
     ws->pixels              = pixels;
-    ws->state.rng           = reinterpret_cast<ulonglong2*>(base + o_rng);
-    ws->state.beta          = reinterpret_cast<float4*>(base + o_beta);
-    ws->state.radiance      = reinterpret_cast<float4*>(base + o_rad);
-    ws->state.prev          = reinterpret_cast<float4*>(base + o_prev);
-    ws->state.flags         = reinterpret_cast<uint32_t*>(base + o_flags);
-    ws->state.ray_o         = reinterpret_cast<float4*>(base + o_ro);
-    ws->state.ray_d         = reinterpret_cast<float4*>(base + o_rd);
-    ws->state.hit           = reinterpret_cast<float4*>(base + o_hit);
-    ws->state.hit_slot      = reinterpret_cast<uint32_t*>(base + o_slot);
-    ws->state.shadow_o      = reinterpret_cast<float4*>(base + o_so);
-    ws->state.shadow_d      = reinterpret_cast<float4*>(base + o_sd);
-    ws->state.shadow_c      = reinterpret_cast<float4*>(base + o_sc);
-    ws->state.segment       = reinterpret_cast<uint32_t*>(base + o_seg);
+    ws->state.view(reinterpret_cast<unsigned char*>(base + o_paths),
+                   reinterpret_cast<unsigned char*>(base + o_shadows), true);
     ws->queues.ext[0]       = reinterpret_cast<uint32_t*>(base + o_e0);
     ws->queues.ext[1]       = reinterpret_cast<uint32_t*>(base + o_e1);
     ws->queues.bins         = reinterpret_cast<uint32_t*>(base + o_bins);

@@ -79,21 +79,64 @@ struct WaveDesc {
     WaveSegment seg[kMaxSegments];
 };
 
-// Structure-of-arrays path state of `capacity` paths (one 16-byte record per field).
+// One field of a record array: element i sits at base + i * STRIDE.
+template <typename T, size_t STRIDE>
+struct RecordField {
+    unsigned char* base = nullptr;  // the field in record 0
+    __host__ __device__ __forceinline__ T& operator[](size_t i) const {
+        return *reinterpret_cast<T*>(base + i * STRIDE);
+    }
+    __host__ __device__ explicit operator bool() const { return base != nullptr; }
+};
+
+// Path state of `capacity` paths as records: one 128-byte path record and one 64-byte shadow
+// record per path slot. Kernels reach paths by slot in queue and bin order, which scatters the
+// slots; a record keeps what one kernel reads of a path in whole 32-byte sectors instead of a
+// 16-byte piece of a sector in each of a dozen arrays. Path record sectors: the ray (ray_o,
+// ray_d: what traversal reads), the hit (hit, hit_slot, flags, segment: what traversal writes),
+// throughput and previous vertex (beta, prev), radiance and RNG (radiance, rng). Shading reads
+// and writes the four; a shadow test reads the shadow record's ray and, when the segment is clear,
+// its contribution and the path's radiance sector.
+constexpr size_t kPathRecordBytes   = 128;
+constexpr size_t kShadowRecordBytes = 64;
+
+template <typename T>
+using PathField = RecordField<T, kPathRecordBytes>;
+template <typename T>
+using ShadowField = RecordField<T, kShadowRecordBytes>;
+
 struct PathState {
-    ulonglong2* rng;       // PCG state, increment
-    float4*     beta;      // throughput, eta scale
-    float4*     radiance;  // accumulated radiance
-    float4*     prev;      // previous scattering vertex, previous pdf
-    uint32_t*   flags;     // bit 0: previous event was delta
-    float4*     ray_o;     // origin, interval minimum
-    float4*     ray_d;     // direction, interval maximum
-    float4*     hit;       // distance, barycentrics (medium: distance, anisotropy)
-    uint32_t*   hit_slot;  // triangle slot, kNone on a miss
-    float4*     shadow_o;  // shadow origin, segment limit
-    float4*     shadow_d;  // shadow direction
-    float4*     shadow_c;  // unoccluded contribution
-    uint32_t*   segment;   // multi-job waves: the path's wave segment
+    PathField<float4>     ray_o;     // origin, interval minimum                        (+0)
+    PathField<float4>     ray_d;     // direction, interval maximum                     (+16)
+    PathField<float4>     hit;       // distance, barycentrics (medium: distance, g)    (+32)
+    PathField<uint32_t>   hit_slot;  // triangle slot, kNone on a miss                  (+48)
+    PathField<uint32_t>   flags;     // bit 0: previous event was delta                 (+52)
+    PathField<uint32_t>   segment;   // multi-job waves: the path's wave segment        (+56)
+    PathField<float4>     beta;      // throughput, eta scale                           (+64)
+    PathField<float4>     prev;      // previous scattering vertex, previous pdf        (+80)
+    PathField<float4>     radiance;  // accumulated radiance                            (+96)
+    PathField<ulonglong2> rng;       // PCG state, increment                            (+112)
+    ShadowField<float4>   shadow_o;  // shadow origin, segment limit                    (+0)
+    ShadowField<float4>   shadow_d;  // shadow direction                                (+16)
+    ShadowField<float4>   shadow_c;  // unoccluded contribution                         (+32)
+
+    // Views of `paths` (capacity x 128 bytes) and `shadows` (capacity x 64 bytes), both
+    // 128-byte aligned. Without `with_segment` the segment field stays unset (single-job use).
+    void view(unsigned char* paths, unsigned char* shadows, bool with_segment) {
+        ray_o.base    = paths + 0;
+        ray_d.base    = paths + 16;
+        hit.base      = paths + 32;
+        hit_slot.base = paths + 48;
+        flags.base    = paths + 52;
+        segment.base  = with_segment ? paths + 56 : nullptr;
+        beta.base     = paths + 64;
+        prev.base     = paths + 80;
+        radiance.base = paths + 96;
+        rng.base      = paths + 112;
+        shadow_o.base = shadows + 0;
+        shadow_d.base = shadows + 16;
+        shadow_c.base = shadows + 32;
+    }
 };
 
 struct Queues {

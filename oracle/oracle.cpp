@@ -37,6 +37,15 @@ namespace oracle {
 constexpr double pi       = std::numbers::pi;
 constexpr double infinity = std::numeric_limits<double>::infinity();
 constexpr double dbl_eps  = std::numeric_limits<double>::epsilon();
+// The unit of the position error bounds that offset spawned rays and shadow-segment ends
+// (path_tracer.cpp:87-105): double's epsilon, as the reference computes them. Built with
+// ORACLE_FP32_OFFSETS it is float's epsilon, the size of the FP32 device's bounds; the tests use
+// that build only to show which image differences come from the larger FP32 offsets.
+#ifdef ORACLE_FP32_OFFSETS
+constexpr double offset_eps = std::numeric_limits<float>::epsilon();
+#else
+constexpr double offset_eps = dbl_eps;
+#endif
 
 // ---- vector helpers (GLM operation order) --------------------------------------------------
 
@@ -1145,7 +1154,7 @@ class SceneBvh {
         result.triangle_index   = primitive.triangle;
         result.primitive        = hit.primitive;
         result.front_face       = dot(ray.direction, geometric) < 0;
-        result.position_error   = absolute_position * (7 * dbl_eps);
+        result.position_error   = absolute_position * (7 * offset_eps);
         return result;
     }
 
@@ -1672,7 +1681,7 @@ class LightSampler {  // light.cpp:197-352
         const double distance  = length(direction);
         const auto   error = (dabs(barycentric.x * light.vertices[0]) + dabs(barycentric.y * light.vertices[1]) +
                             dabs(barycentric.z * light.vertices[2])) *
-                           (7 * dbl_eps);
+                           (7 * offset_eps);
         LightSample s;
         s.direction      = direction / distance;
         s.radiance       = light.radiance;

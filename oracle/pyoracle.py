@@ -37,12 +37,16 @@ _lib = None
 
 def lib():
     """The oracle library: liboracle.so (nofma without hardware FMA), or the variant the
-    environment names in ORACLE_VARIANT ("contract": multiply-adds fused by the compiler)."""
+    environment names in ORACLE_VARIANT ("contract": multiply-adds fused by the compiler;
+    "f32offsets": ray offsets sized with float's epsilon, as on the FP32 device)."""
     global _lib
     if _lib is None:
         name = "liboracle.so" if _cpu_has_fma() else "liboracle_nofma.so"
-        if os.environ.get("ORACLE_VARIANT") == "contract":
+        variant = os.environ.get("ORACLE_VARIANT")
+        if variant == "contract":
             name = "liboracle_contract.so"
+        elif variant == "f32offsets":
+            name = "liboracle_f32offsets.so"
         path = os.path.join(BUILD, name)
         if not os.path.exists(path):
             build()

@@ -118,8 +118,9 @@ def compare_nearest(g_prim, c_hit, c_prim, tris, origins, dirs, tmin, tmax, limi
     """
     g_hit = g_prim != 0xFFFFFFFF
     c_hit = np.asarray(c_hit, bool)
-    c_prim = np.where(c_hit, np.asarray(c_prim), -1).astype(np.int64)
-    g_prim64 = np.where(g_hit, g_prim, -1).astype(np.int64)
+    # Widen before substituting -1: NumPy casts a Python -1 to the array's uint32 otherwise.
+    c_prim = np.where(c_hit, np.asarray(c_prim).astype(np.int64), -1)
+    g_prim64 = np.where(g_hit, np.asarray(g_prim).astype(np.int64), -1)
     differ = np.flatnonzero((g_hit != c_hit) | (g_prim64 != c_prim))
     classes = {"tie": 0, "graze": 0, "interval": 0, "unexplained": 0}
     examples = []

@@ -40,6 +40,8 @@ SCENES = {
     "room": lambda: sc.job_scene(60_000, 12),
     "spheres": lambda: sc.sphere_field(40, 10.0, 9, 3, variants=5),
     "transforms": mirrored_and_scaled,
+    # more instances than one 128-thread block of the per-instance kernels
+    "many": lambda: sc.sphere_field(700, 40.0, 13, 1, variants=6),
 }
 
 
