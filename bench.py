@@ -80,9 +80,9 @@ def parse():
                    help="Poisson arrival rate of the serving run, jobs per second")
     p.add_argument("--leg", choices=["serve", "stress"], default=None,
                    help="run one secondary workload alone and print its JSON line")
-    p.add_argument("--stress", action="store_true",
-                   help="also render the 20M-triangle scene in a medium at 3840x2160, 256 spp, "
-                        "depth 16 (about half a minute)")
+    p.add_argument("--no-stress", dest="stress", action="store_false",
+                   help="skip the 20M-triangle scene in a medium at 3840x2160, 256 spp, depth 16 "
+                        "(about half a minute; rendered by default at N=1)")
     # Profiling aids (ncu captures); the defaults are the benchmark.
     p.add_argument("--jobs", type=int, default=JOBS, help="render only the first J jobs")
     p.add_argument("--no-autotune", action="store_true", help="default wave shape, no tuning")

@@ -43,13 +43,18 @@ MR_HD f3 transform_point(const float* m, float x, float y, float z) {
     return {row(0), row(1), row(2)};
 }
 
-// normalize(normal_to_world * n) of a mesh corner normal (src/render/bvh.cpp:319-320), with the
-// multiply-adds fused explicitly so every kernel that evaluates it gets the same bits.
+// normalize(normal_to_world * n) of a mesh corner normal (src/render/bvh.cpp:319-320). Every
+// operation is rounded explicitly (fused multiply-adds for the product, then a squared length,
+// square root and reciprocal with no contraction), so the flattening, which stores these
+// normals, and a two-level scene, which evaluates them at each hit in another kernel, get the
+// same bits whatever the compiler fuses around them.
 __device__ __forceinline__ f3 world_normal(const float* m, const float* n) {
-    const f3 w = {fmaf(m[6], n[2], fmaf(m[3], n[1], m[0] * n[0])),
-                  fmaf(m[7], n[2], fmaf(m[4], n[1], m[1] * n[0])),
-                  fmaf(m[8], n[2], fmaf(m[5], n[1], m[2] * n[0]))};
-    return normalize(w);
+    const f3 w = {fmaf(m[6], n[2], fmaf(m[3], n[1], __fmul_rn(m[0], n[0]))),
+                  fmaf(m[7], n[2], fmaf(m[4], n[1], __fmul_rn(m[1], n[0]))),
+                  fmaf(m[8], n[2], fmaf(m[5], n[1], __fmul_rn(m[2], n[0])))};
+    const float length2 = __fadd_rn(__fadd_rn(__fmul_rn(w.x, w.x), __fmul_rn(w.y, w.y)), __fmul_rn(w.z, w.z));
+    const float inverse = __fdiv_rn(1.0f, __fsqrt_rn(length2));
+    return {__fmul_rn(w.x, inverse), __fmul_rn(w.y, inverse), __fmul_rn(w.z, inverse)};
 }
 
 enum TriFlags : unsigned {

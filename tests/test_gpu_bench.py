@@ -1,5 +1,5 @@
 """bench.py's own arm on the GPU prints one JSON line with the contract's keys: run on four jobs
-of the mix with the default wave shape, one timed step, no serving, e2e or CPU legs. The
+of the mix with the default wave shape, one timed step, no serving, e2e, CPU or stress legs. The
 secondary legs (per-quintile batched vs plain, config 1, the 1080p frame) report."""
 
 import json
@@ -17,7 +17,8 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 def test_bench_prints_the_contract_line():
     result = subprocess.run([sys.executable, "bench.py", "--steps", "1", "--warmup", "3",
                              "--jobs", "4", "--no-autotune", "--no-serve", "--no-e2e",
-                             "--no-cpu-baseline"], cwd=ROOT, capture_output=True, text=True,
+                             "--no-cpu-baseline", "--no-stress"], cwd=ROOT, capture_output=True,
+                            text=True,
                             timeout=900)
     assert result.returncode == 0, result.stderr[-4000:]
     line = json.loads(result.stdout.strip().splitlines()[-1])
