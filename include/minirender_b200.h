@@ -435,7 +435,7 @@ mr_status mr_capture_shadow_rays(const mr_scene* scene, const mr_integrator_sett
  * allocation-free form of mr_trace_paths (same per-path results). `device_rays`, `device_keys`
  * (seed, pixel, sample per path) and `device_radiance` (3 floats per path) are device memory;
  * `stream` is a cudaStream_t (null = legacy default stream); the call returns after the work
- * has finished. The working memory is one fixed array of about 4.2 MB inside the library, held
+ * has finished. The working memory is one fixed array of about 4.3 MB inside the library, held
  * on every GPU that loads it until the process exits. The first call on a device looks up the
  * array's address, which under CUDA's lazy module loading also loads the module and places the
  * array in device memory (an allocation and a synchronisation): warm up each device with a call

@@ -3,8 +3,9 @@
     python -m minirender_b200.build [--verbose]
 
 Each CUDA source under csrc/ is compiled to an object under _build/ (in parallel, skipped when
-up to date) and linked into minirender_b200/libminirender_b200.so. Host code is compiled with
--ffp-contract=off so that host and device flatten scene geometry with the same roundings.
+up to date) and linked into minirender_b200/libminirender_b200.so. Device code is compiled with
+-fmad=false and host code with -ffp-contract=off: only the multiply-adds the source fuses
+explicitly are fused, so host and device, and every kernel, round the same expression alike.
 """
 
 from __future__ import annotations
@@ -22,7 +23,11 @@ BUILD = os.path.join(ROOT, "_build", "minirender_b200")
 OUTPUT = os.path.join(HERE, "libminirender_b200.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
+# -fmad=false: no multiply-add is fused unless the source fuses it (fmaf, __fmaf_rn). Every
+# kernel that evaluates the same expression then rounds it the same way, whatever its register
+# budget or inlining context, so images are bitwise equal across the plain, batched, two-level
+# and allocation-free entry points.
+FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-fmad=false",
          "-Xcompiler", "-fPIC,-ffp-contract=off,-Wall", "-Xptxas", "-warn-spills"]
 
 

@@ -125,7 +125,7 @@ struct Lane {
     std::shared_ptr<Workspace>                           ws;
     WaveDesc*                                            d_wave = nullptr;
     cudaEvent_t                                          mark   = nullptr;
-    std::map<std::pair<uint32_t, int>, cudaGraphExec_t> graphs;  // by depth, media | two levels << 1
+    std::map<std::pair<uint32_t, int>, cudaGraphExec_t> graphs;  // by depth, media | two levels << 1 | ray sort << 2
 };
 
 // Mean of the samples accumulated so far (preview of a running job): pixels in rows < row have
@@ -620,8 +620,8 @@ class Server {
         return true;
     }
 
-    cudaGraphExec_t graph_for(Lane& lane, uint32_t depth, bool media, bool two) {
-        const auto key = std::make_pair(depth, (media ? 1 : 0) | (two ? 2 : 0));
+    cudaGraphExec_t graph_for(Lane& lane, uint32_t depth, bool media, bool two, bool ray_sort) {
+        const auto key = std::make_pair(depth, (media ? 1 : 0) | (two ? 2 : 0) | (ray_sort ? 4 : 0));
         auto it = lane.graphs.find(key);
         if (it != lane.graphs.end()) {
             return it->second;
@@ -629,7 +629,8 @@ class Server {
         cudaGraph_t graph = nullptr;
         MR_CUDA(cudaStreamBeginCapture(lane.stream, cudaStreamCaptureModeThreadLocal));
         try {
-            Engine::enqueue_batch_paths(lane.d_wave, depth, media, two, shape_, *lane.ws, lane.stream);
+            Engine::enqueue_batch_paths(lane.d_wave, depth, media, two, ray_sort, shape_, *lane.ws,
+                                        lane.stream);
         } catch (...) {
             cudaStreamEndCapture(lane.stream, &graph);
             if (graph) {
@@ -729,11 +730,14 @@ class Server {
         MR_CUDA(cudaStreamWaitEvent(lane.stream, admin_ready_, 0));
         MR_CUDA(cudaMemcpyAsync(lane.d_wave, &h, bytes, cudaMemcpyHostToDevice, lane.stream));
         MR_CUDA(cudaEventRecord(rec.start, lane.stream));
+        // Large waves sort each bounce's extension rays by origin cell and direction.
+        const bool ray_sort = count >= kRaySortMinPaths;
         if (settings_.batch.use_graphs) {
-            MR_CUDA(cudaGraphLaunch(graph_for(lane, depth, media, two), lane.stream));
+            MR_CUDA(cudaGraphLaunch(graph_for(lane, depth, media, two, ray_sort), lane.stream));
             ++stats_.graph_launches;
         } else {
-            Engine::enqueue_batch_paths(lane.d_wave, depth, media, two, shape_, *lane.ws, lane.stream);
+            Engine::enqueue_batch_paths(lane.d_wave, depth, media, two, ray_sort, shape_, *lane.ws,
+                                        lane.stream);
         }
         // Resolves run in wave order across lanes: per pixel, samples accumulate in order.
         MR_CUDA(cudaStreamWaitEvent(lane.stream, resolve_chain_, 0));
@@ -742,7 +746,7 @@ class Server {
         MR_CUDA(cudaMemcpyAsync(h_errors_[stage], d_errors_, settings_.max_jobs * sizeof(unsigned),
                                 cudaMemcpyDeviceToHost, lane.stream));
         MR_CUDA(cudaEventRecord(rec.done, lane.stream));
-        const uint64_t launches = Engine::batch_wave_launches(depth);
+        const uint64_t launches = Engine::batch_wave_launches(depth, ray_sort);
         note_launches(launches);
         stats_.kernel_launches += launches;
         stats_.segments += n;

@@ -6,7 +6,7 @@
 // host loop that must not risk the implicit device synchronisation an allocation can cause.
 // This entry point gives them the same per-path results as mr_trace_paths with zero
 // allocations: the wavefront's path state, queues, counters and a staging copy of the rays live
-// in `g_trace_scratch` (about 4.2 MB, resident on every device that loads the library until the
+// in `g_trace_scratch` (about 4.3 MB, resident on every device that loads the library until the
 // process exits). Inputs and outputs stay in the caller's device memory.
 //
 // The array's device address is resolved once per device with cudaGetSymbolAddress (the name in

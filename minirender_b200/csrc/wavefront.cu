@@ -39,12 +39,13 @@ struct KernelArgs {
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31; }
 
 // Appends `value` to queue[key] (key == kNone: nothing) with one atomic per distinct key per
-// warp. Must be called by all 32 lanes.
-__device__ __forceinline__ void warp_append(uint32_t key, uint32_t value, uint32_t* counts,
-                                            uint32_t* queues, size_t stride) {
+// warp and returns its position in that queue (kNone when nothing was appended). Must be called
+// by all 32 lanes.
+__device__ __forceinline__ uint32_t warp_append(uint32_t key, uint32_t value, uint32_t* counts,
+                                                uint32_t* queues, size_t stride) {
     const unsigned peers = __match_any_sync(0xffffffffu, key);
     if (key == kNone) {
-        return;
+        return kNone;
     }
     const int lane   = lane_id();
     const int leader = __ffs(peers) - 1;
@@ -55,6 +56,7 @@ __device__ __forceinline__ void warp_append(uint32_t key, uint32_t value, uint32
     base               = __shfl_sync(peers, base, leader);
     const uint32_t pos = base + __popc(peers & ((1u << lane) - 1u));
     queues[key * stride + pos] = value;
+    return pos;
 }
 
 __device__ __forceinline__ void warp_add_stat(unsigned long long* stat, uint32_t value) {
@@ -381,9 +383,29 @@ __global__ void __launch_bounds__(128, TWO ? 5 : 8) trace_kernel(KernelArgs a) {
 // ---- shade ----
 
 struct ShadeResult {
-    bool continue_path;
-    bool shadow;
+    bool     continue_path;
+    bool     shadow;
+    uint32_t sort_key;  // coherence key of the continuing ray
 };
+
+// Coherence key of a ray: the Morton code of its origin's cell in the scene's bounds
+// (kSortAxisBits per axis), then its direction octant. Rays with equal keys start in the same
+// region heading the same way, so they visit much of the same tree.
+__device__ __forceinline__ uint32_t coherence_key(const DeviceScene& s, f3 origin, f3 direction) {
+    constexpr float cells = static_cast<float>(1u << kSortAxisBits);
+    uint32_t        morton = 0;
+    for (int k = 0; k < 3; ++k) {
+        const float extent = s.root_hi[k] - s.root_lo[k];
+        const float u      = extent > 0 ? (comp(origin, k) - s.root_lo[k]) * (cells / extent) : 0.0f;
+        const uint32_t c   = static_cast<uint32_t>(fminf(fmaxf(u, 0.0f), cells - 1.0f));
+        for (int bit = 0; bit < kSortAxisBits; ++bit) {
+            morton |= ((c >> bit) & 1u) << (3 * bit + k);
+        }
+    }
+    const uint32_t octant = (direction.x < 0 ? 1u : 0u) | (direction.y < 0 ? 2u : 0u) |
+                            (direction.z < 0 ? 4u : 0u);
+    return morton << 3 | octant;
+}
 
 __device__ __forceinline__ float emission_weight(const IntegratorParams& p, uint32_t depth,
                                                  bool previous_delta, float previous_pdf,
@@ -429,7 +451,7 @@ __device__ ShadeResult shade_surface(const KernelArgs& a, uint32_t path, int bin
     const bool              previous_delta = a.st.flags[path] & 1u;
     float4                  L4    = a.st.radiance[path];
     f3                      L     = xyz(L4);
-    ShadeResult             out{false, false};
+    ShadeResult             out{false, false, 0u};
 
     if (bin == kBinMiss) {
         L += beta * environment_radiance(s, dir) *
@@ -486,6 +508,7 @@ __device__ ShadeResult shade_surface(const KernelArgs& a, uint32_t path, int bin
         a.st.beta[path]  = f4(beta, eta_scale);
         store_rng(a.st, path, rng);
         out.continue_path = true;
+        out.sort_key      = a.q.staging ? coherence_key(s, vertex, next) : 0u;
         return out;
     }
 
@@ -582,6 +605,7 @@ __device__ ShadeResult shade_surface(const KernelArgs& a, uint32_t path, int bin
     a.st.beta[path]  = f4(beta, eta_scale);
     store_rng(a.st, path, rng);
     out.continue_path = true;
+    out.sort_key      = a.q.staging ? coherence_key(s, origin, next) : 0u;
     return out;
 }
 
@@ -603,7 +627,7 @@ __global__ void __launch_bounds__(128) shade_kernel(KernelArgs a) {
     for (uint32_t base = warp * 32; base < total; base += warps * 32) {
         const uint32_t i      = base + lane_id();
         uint32_t       path   = 0;
-        uint32_t       ext_key = kNone, shadow_key = kNone;
+        uint32_t       ext_key = kNone, shadow_key = kNone, sort_key = kNone;
         if (i < total) {
             int bin = 0;
             while (i >= prefix[bin + 1]) {
@@ -615,9 +639,23 @@ __global__ void __launch_bounds__(128) shade_kernel(KernelArgs a) {
             note_error<BATCH>(segment_of<BATCH>(a, path), e, error);
             ext_key              = r.continue_path ? 0u : kNone;
             shadow_key           = r.shadow ? 0u : kNone;
+            sort_key             = r.continue_path ? r.sort_key : kNone;
         }
         warp_append(shadow_key, path, &ctr->shadow, a.q.shadow, 0);
-        warp_append(ext_key, path, &nctr->ext, next, 0);
+        if (a.q.staging) {
+            // Staged for the coherence sort: the path at its position, its key beside it, and
+            // one count per distinct key per warp.
+            const uint32_t pos = warp_append(ext_key, path, &nctr->ext, a.q.staging, 0);
+            if (ext_key != kNone) {
+                a.q.keys[pos] = sort_key;
+            }
+            const unsigned same = __match_any_sync(0xffffffffu, sort_key);
+            if (sort_key != kNone && lane_id() == __ffs(same) - 1) {
+                atomicAdd(a.q.buckets + sort_key, static_cast<uint32_t>(__popc(same)));
+            }
+        } else {
+            warp_append(ext_key, path, &nctr->ext, next, 0);
+        }
     }
     warp_add_stat(a.q.stats + kStatShadowRays, stats.shadow_rays);
     warp_add_stat(a.q.stats + kStatScattering, stats.scattering);
@@ -625,6 +663,58 @@ __global__ void __launch_bounds__(128) shade_kernel(KernelArgs a) {
     warp_add_stat(a.q.stats + kStatMedium, stats.medium);
     if (error) {
         atomicOr(a.q.error, error);
+    }
+}
+
+// ---- coherence sort of the next bounce's extension rays ----
+
+// Exclusive scan of the bucket counts into the cursors, by one block of 1024 threads; the counts
+// are cleared for the next bounce.
+__global__ void __launch_bounds__(1024) sort_scan_kernel(uint32_t* buckets) {
+    constexpr uint32_t per = kSortBuckets / 1024;
+    __shared__ uint32_t partial[1024];
+    const uint32_t      t = threadIdx.x;
+    uint32_t            local[per];
+    uint32_t            sum = 0;
+    for (uint32_t k = 0; k < per; ++k) {
+        local[k]             = buckets[t * per + k];
+        buckets[t * per + k] = 0;
+        sum += local[k];
+    }
+    partial[t] = sum;
+    __syncthreads();
+    for (uint32_t offset = 1; offset < 1024; offset <<= 1) {
+        const uint32_t v = t >= offset ? partial[t - offset] : 0u;
+        __syncthreads();
+        partial[t] += v;
+        __syncthreads();
+    }
+    uint32_t run = partial[t] - sum;
+    for (uint32_t k = 0; k < per; ++k) {
+        buckets[kSortBuckets + t * per + k] = run;
+        run += local[k];
+    }
+}
+
+// Moves the staged paths into the next bounce's queue in key order (within a key, in the order
+// the warps claim their places: path results do not depend on queue order).
+__global__ void sort_scatter_kernel(KernelArgs a) {
+    const uint32_t n    = a.q.counters[a.bounce + 1].ext;
+    uint32_t*      next = a.q.ext[(a.bounce + 1) & 1];
+    const uint32_t step = gridDim.x * blockDim.x;
+    for (uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u; base < n; base += step) {
+        const uint32_t i    = base + lane_id();
+        const uint32_t key  = i < n ? a.q.keys[i] : kNone;
+        const unsigned same = __match_any_sync(0xffffffffu, key);
+        if (key != kNone) {
+            const int leader = __ffs(same) - 1;
+            uint32_t  pos    = 0;
+            if (lane_id() == leader) {
+                pos = atomicAdd(a.q.buckets + kSortBuckets + key, static_cast<uint32_t>(__popc(same)));
+            }
+            pos       = __shfl_sync(same, pos, leader) + __popc(same & ((1u << lane_id()) - 1u));
+            next[pos] = a.q.staging[i];
+        }
     }
 }
 
@@ -822,6 +912,9 @@ std::shared_ptr<Workspace> allocate_workspace(size_t capacity, uint32_t max_boun
     const size_t o_e1 = field(capacity * sizeof(uint32_t));
     const size_t o_bins = field(capacity * kBinCount * sizeof(uint32_t));
     const size_t o_shadow = field(capacity * sizeof(uint32_t));
+    const size_t o_stage = field(capacity * sizeof(uint32_t));
+    const size_t o_keys  = field(capacity * sizeof(uint32_t));
+    const size_t o_buck  = field(2 * kSortBuckets * sizeof(uint32_t));
     const size_t o_ctr = field((max_bounces + 2) * sizeof(BounceCounters));
     const size_t o_stats = field(kStatCount * sizeof(unsigned long long));
     const size_t o_err = field(sizeof(unsigned));
@@ -840,6 +933,10 @@ std::shared_ptr<Workspace> allocate_workspace(size_t capacity, uint32_t max_boun
     ws->queues.ext[1]       = reinterpret_cast<uint32_t*>(base + o_e1);
     ws->queues.bins         = reinterpret_cast<uint32_t*>(base + o_bins);
     ws->queues.shadow       = reinterpret_cast<uint32_t*>(base + o_shadow);
+    ws->queues.staging      = reinterpret_cast<uint32_t*>(base + o_stage);
+    ws->queues.keys         = reinterpret_cast<uint32_t*>(base + o_keys);
+    ws->queues.buckets      = reinterpret_cast<uint32_t*>(base + o_buck);
+    MR_CUDA(cudaMemset(ws->queues.buckets, 0, kSortBuckets * sizeof(uint32_t)));  // counts start at 0
     ws->queues.counters     = reinterpret_cast<BounceCounters*>(base + o_ctr);
     ws->queues.stats        = reinterpret_cast<unsigned long long*>(base + o_stats);
     ws->queues.error        = reinterpret_cast<unsigned*>(base + o_err);
@@ -987,10 +1084,17 @@ void Engine::run_wave(const Scene& scene, const IntegratorParams& params, const 
     const LaunchShape& shape = launch_shape();
     const bool         media = scene.d.medium_count > 0;
     const bool         two   = scene.d.two_level != 0;
+    // Large waves sort each bounce's extension rays by origin cell and direction; small ones
+    // keep their order (the sort's fixed cost would outweigh the coherence it buys).
+    const bool         ray_sort = ws.queues.staging != nullptr && init.count >= kRaySortMinPaths;
+    if (!ray_sort) {
+        a.q.staging = nullptr;
+    }
     KernelTiming&      timing = kernel_timing();
     bool               timed  = false;
     timed = timing.enabled.load();
-    note_launches(1 + 2ull * (params.maximum_depth + 1) + (init.capture ? 1 : 0));
+    note_launches(1 + 2ull * (params.maximum_depth + 1) + (ray_sort ? 2ull * params.maximum_depth : 0ull) +
+                  (init.capture ? 1 : 0));
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
     // The timed launches are the trace kernels: nearest-hit and shadow tests both count.
     unsigned long long before[4] = {0, 0, 0, 0};
@@ -1025,6 +1129,10 @@ void Engine::run_wave(const Scene& scene, const IntegratorParams& params, const 
             shade_kernel<false, true><<<shape.shade_blocks_two, 128, 0, stream>>>(a);
         } else {
             shade_kernel<false, false><<<shape.shade_blocks, 128, 0, stream>>>(a);
+        }
+        if (ray_sort && bounce < params.maximum_depth) {
+            sort_scan_kernel<<<1, 1024, 0, stream>>>(a.q.buckets);
+            sort_scatter_kernel<<<shape.shade_blocks, 128, 0, stream>>>(a);
         }
         if (bounce == 0 && init.capture) {
             capture_shadow_kernel<<<(init.count + 127) / 128, 128, 0, stream>>>(a, init.capture->rays,
@@ -1065,7 +1173,8 @@ void Engine::batch_occupancy(int& trace_blocks_per_sm, int& shade_blocks_per_sm)
 }
 
 void Engine::enqueue_batch_paths(const WaveDesc* wave, uint32_t maximum_depth, bool media, bool two,
-                                 const BatchShape& shape, Workspace& ws, cudaStream_t stream) {
+                                 bool ray_sort, const BatchShape& shape, Workspace& ws,
+                                 cudaStream_t stream) {
     if (maximum_depth + 1 > ws.max_bounces || !ws.state.segment) {
         fail(MR_LENGTH_ERROR, "Wave exceeds the workspace capacity");
     }
@@ -1078,6 +1187,10 @@ void Engine::enqueue_batch_paths(const WaveDesc* wave, uint32_t maximum_depth, b
     a.capacity     = static_cast<uint32_t>(ws.capacity);
     a.occluded_out = nullptr;
     a.wave         = wave;
+    ray_sort       = ray_sort && ws.queues.staging != nullptr;
+    if (!ray_sort) {
+        a.q.staging = nullptr;
+    }
     // The two-level variants keep fewer blocks resident (more registers per thread): their grid
     // is capped at what fits, the persistent loop takes the work either way.
     int trace_blocks = shape.trace_blocks;
@@ -1101,6 +1214,10 @@ void Engine::enqueue_batch_paths(const WaveDesc* wave, uint32_t maximum_depth, b
             shade_kernel<true, true><<<shape.shade_blocks, 128, 0, stream>>>(a);
         } else {
             shade_kernel<true, false><<<shape.shade_blocks, 128, 0, stream>>>(a);
+        }
+        if (ray_sort && bounce < maximum_depth) {
+            sort_scan_kernel<<<1, 1024, 0, stream>>>(a.q.buckets);
+            sort_scatter_kernel<<<shape.shade_blocks, 128, 0, stream>>>(a);
         }
     }
     MR_CUDA(cudaGetLastError());

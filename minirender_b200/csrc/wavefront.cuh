@@ -139,8 +139,18 @@ struct PathState {
     }
 };
 
+// Coherence sort of the extension rays between bounces: a counting sort on a key made of the
+// Morton code of the ray origin's cell (kSortAxisBits per axis, in the scene's bounds) and the
+// direction octant. Waves of fewer paths than kRaySortMinPaths are not sorted.
+constexpr int      kSortAxisBits    = 4;
+constexpr uint32_t kSortBuckets     = 8u << (3 * kSortAxisBits);
+constexpr uint32_t kRaySortMinPaths = 1u << 18;
+
 struct Queues {
     uint32_t*       ext[2];
+    uint32_t*       staging;  // this bounce's continuing paths before the sort (null: no sort)
+    uint32_t*       keys;     // their sort keys, at the same positions
+    uint32_t*       buckets;  // kSortBuckets counts, then kSortBuckets cursors
     uint32_t*       bins;    // kBinCount * capacity
     uint32_t*       shadow;
     BounceCounters* counters;  // maximum_depth + 2 entries
@@ -209,7 +219,8 @@ class Engine {
     // per path. The launch sequence depends only on its arguments, so it can be captured once in
     // a CUDA graph and replayed for every wave of the same depth.
     static void enqueue_batch_paths(const WaveDesc* wave, uint32_t maximum_depth, bool media, bool two,
-                                    const BatchShape& shape, Workspace& ws, cudaStream_t stream);
+                                    bool ray_sort, const BatchShape& shape, Workspace& ws,
+                                    cudaStream_t stream);
 
     // Enqueues the per-pixel resolve of a wave's radiance into each job's accumulator and image.
     static void enqueue_batch_resolve(const WaveDesc* wave, Workspace& ws, cudaStream_t stream);
@@ -218,7 +229,9 @@ class Engine {
     static void batch_occupancy(int& trace_blocks_per_sm, int& shade_blocks_per_sm);
 
     // Kernel launches of one wave (paths + resolve).
-    static uint64_t batch_wave_launches(uint32_t maximum_depth) { return 2ull + 2ull * (maximum_depth + 1); }
+    static uint64_t batch_wave_launches(uint32_t maximum_depth, bool ray_sort) {
+        return 2ull + 2ull * (maximum_depth + 1) + (ray_sort ? 2ull * maximum_depth : 0ull);
+    }
 };
 
 // Workspace pool (per device).

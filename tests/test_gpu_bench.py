@@ -44,6 +44,7 @@ def test_bench_prints_the_contract_line():
     assert "error" not in preview, preview
     assert preview["batched"] > 0 and preview["plain"] > 0
     assert all(q["batched_vs_plain"] > 0 for q in line["config"]["quintiles"])
+    assert line["config"]["batched_vs_plain_bound"]["value"] > 0
     c1 = line["config"]["config1"]
     assert c1["value"] > 0 and c1["e2e"]["value"] > 0
     assert line["config"]["large_frame"]["value"] > 0
