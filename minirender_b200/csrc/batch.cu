@@ -669,7 +669,7 @@ class Server {
         WaveRecord     rec;
         rec.stage            = stage;
         uint64_t space       = settings_.batch.wave_paths;
-        uint32_t count = 0, pixels = 0, depth = 0;
+        uint32_t count = 0, pixels = 0, depth = 0, slots = 0;
         bool     media = false, two = false;
         for (Job* j : order) {
             if (rec.pieces.size() == kMaxSegments || space < 32) {
@@ -699,6 +699,7 @@ class Server {
             depth = std::max(depth, j->p.maximum_depth);
             media = media || j->scene->d.medium_count > 0;
             two   = two || j->scene->d.two_level != 0;
+            slots = std::max(slots, j->scene->d.slot_count);
             j->issued = after;
             j->issued_samples += paths;
             rec.pieces.push_back({j, after, paths, after.sample >= j->spp});
@@ -730,8 +731,9 @@ class Server {
         MR_CUDA(cudaStreamWaitEvent(lane.stream, admin_ready_, 0));
         MR_CUDA(cudaMemcpyAsync(lane.d_wave, &h, bytes, cudaMemcpyHostToDevice, lane.stream));
         MR_CUDA(cudaEventRecord(rec.start, lane.stream));
-        // Large waves sort each bounce's extension rays by origin cell and direction.
-        const bool ray_sort = count >= kRaySortMinPaths;
+        // Large waves of scenes whose traversal is not trivial sort each bounce's extension rays
+        // by where they start and their direction.
+        const bool ray_sort = count >= kRaySortMinPaths && slots >= kRaySortMinSlots;
         if (settings_.batch.use_graphs) {
             MR_CUDA(cudaGraphLaunch(graph_for(lane, depth, media, two, ray_sort), lane.stream));
             ++stats_.graph_launches;

@@ -163,6 +163,7 @@ struct DeviceScene {
     int                   has_nodes;        // 0 for an empty scene
     uint32_t              node_count;
     uint32_t              primitive_count;
+    uint32_t              slot_count;       // triangle slots in leaf order (two-level: primitives)
     uint32_t              light_count;
     int                   environment_choice;  // light index of the environment, -1 if none
     f3                    environment;

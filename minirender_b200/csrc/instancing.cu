@@ -513,6 +513,7 @@ void build_instance_tree(Scene& scene, cudaStream_t stream) {
 void publish_two_level(Scene& scene) {
     auto& t                  = *scene.two;
     scene.d.two_level        = 1;
+    scene.d.slot_count       = scene.d.primitive_count;
     scene.d.instance_count   = static_cast<uint32_t>(t.host_instances.size());
     scene.d.instances        = t.instances.ptr;
     scene.d.tlas_items       = t.tlas_items.ptr;

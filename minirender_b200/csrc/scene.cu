@@ -815,6 +815,7 @@ std::unique_ptr<Scene> create_scene(const mr_scene_desc& desc, const mr_bvh_desc
             scene->nodes  = std::move(wide.nodes);
             wide_count    = wide.count;
             scene->tris.allocate(3ull * slots);
+            scene->d.slot_count = slots;
             gather_triangles_kernel<<<(slots + 255) / 256, 256, 0, stream>>>(world.ptr, ref_order.ptr, slots,
                                                                              scene->tris.ptr);
             mark_leaf_end_kernel<<<(node_count + 255) / 256, 256, 0, stream>>>(ref_nodes.ptr, node_count,

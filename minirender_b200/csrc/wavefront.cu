@@ -388,23 +388,31 @@ struct ShadeResult {
     uint32_t sort_key;  // coherence key of the continuing ray
 };
 
-// Coherence key of a ray: the Morton code of its origin's cell in the scene's bounds
-// (kSortAxisBits per axis), then its direction octant. Rays with equal keys start in the same
-// region heading the same way, so they visit much of the same tree.
-__device__ __forceinline__ uint32_t coherence_key(const DeviceScene& s, f3 origin, f3 direction) {
-    constexpr float cells = static_cast<float>(1u << kSortAxisBits);
-    uint32_t        morton = 0;
-    for (int k = 0; k < 3; ++k) {
-        const float extent = s.root_hi[k] - s.root_lo[k];
-        const float u      = extent > 0 ? (comp(origin, k) - s.root_lo[k]) * (cells / extent) : 0.0f;
-        const uint32_t c   = static_cast<uint32_t>(fminf(fmaxf(u, 0.0f), cells - 1.0f));
-        for (int bit = 0; bit < kSortAxisBits; ++bit) {
-            morton |= ((c >> bit) & 1u) << (3 * bit + k);
+// Coherence key of a ray: where it starts, then its direction octant. A ray leaving a surface
+// (`slot` its triangle's slot) takes the slot's range in leaf order; a ray leaving a medium vertex
+// (`slot` kNone) the Morton code of its origin's cell in the scene's bounds (kSortAxisBits per
+// axis). Rays with equal keys start near one another heading the same way, so they visit much of
+// the same tree.
+__device__ __forceinline__ uint32_t coherence_key(const DeviceScene& s, uint32_t slot, f3 origin,
+                                                  f3 direction) {
+    uint32_t cell = 0;
+    if (slot != kNone && s.slot_count > 0) {
+        cell = static_cast<uint32_t>((static_cast<uint64_t>(slot) * kSortCells) / s.slot_count);
+        cell = min(cell, kSortCells - 1);
+    } else {
+        constexpr float cells = static_cast<float>(1u << kSortAxisBits);
+        for (int k = 0; k < 3; ++k) {
+            const float extent = s.root_hi[k] - s.root_lo[k];
+            const float u      = extent > 0 ? (comp(origin, k) - s.root_lo[k]) * (cells / extent) : 0.0f;
+            const uint32_t c   = static_cast<uint32_t>(fminf(fmaxf(u, 0.0f), cells - 1.0f));
+            for (int bit = 0; bit < kSortAxisBits; ++bit) {
+                cell |= ((c >> bit) & 1u) << (3 * bit + k);
+            }
         }
     }
     const uint32_t octant = (direction.x < 0 ? 1u : 0u) | (direction.y < 0 ? 2u : 0u) |
                             (direction.z < 0 ? 4u : 0u);
-    return morton << 3 | octant;
+    return cell << 3 | octant;
 }
 
 __device__ __forceinline__ float emission_weight(const IntegratorParams& p, uint32_t depth,
@@ -508,7 +516,7 @@ __device__ ShadeResult shade_surface(const KernelArgs& a, uint32_t path, int bin
         a.st.beta[path]  = f4(beta, eta_scale);
         store_rng(a.st, path, rng);
         out.continue_path = true;
-        out.sort_key      = a.q.staging ? coherence_key(s, vertex, next) : 0u;
+        out.sort_key      = a.q.staging ? coherence_key(s, kNone, vertex, next) : 0u;
         return out;
     }
 
@@ -605,7 +613,7 @@ __device__ ShadeResult shade_surface(const KernelArgs& a, uint32_t path, int bin
     a.st.beta[path]  = f4(beta, eta_scale);
     store_rng(a.st, path, rng);
     out.continue_path = true;
-    out.sort_key      = a.q.staging ? coherence_key(s, origin, next) : 0u;
+    out.sort_key      = a.q.staging ? coherence_key(s, slot, origin, next) : 0u;
     return out;
 }
 
@@ -1086,7 +1094,8 @@ void Engine::run_wave(const Scene& scene, const IntegratorParams& params, const 
     const bool         two   = scene.d.two_level != 0;
     // Large waves sort each bounce's extension rays by origin cell and direction; small ones
     // keep their order (the sort's fixed cost would outweigh the coherence it buys).
-    const bool         ray_sort = ws.queues.staging != nullptr && init.count >= kRaySortMinPaths;
+    const bool         ray_sort = ws.queues.staging != nullptr && init.count >= kRaySortMinPaths &&
+                                  scene.d.slot_count >= kRaySortMinSlots;
     if (!ray_sort) {
         a.q.staging = nullptr;
     }

@@ -139,12 +139,18 @@ struct PathState {
     }
 };
 
-// Coherence sort of the extension rays between bounces: a counting sort on a key made of the
-// Morton code of the ray origin's cell (kSortAxisBits per axis, in the scene's bounds) and the
-// direction octant. Waves of fewer paths than kRaySortMinPaths are not sorted.
+// Coherence sort of the extension rays between bounces: a counting sort on a key made of where
+// the ray starts (the position of its origin's triangle in the tree's leaf order, in 4,096 equal
+// ranges; or, for a medium vertex, the Morton code of its cell in the scene's bounds) and its
+// direction octant. Leaf order follows the tree, so a range covers a compact piece of geometry
+// however the geometry is spread. Waves of fewer paths than kRaySortMinPaths and scenes of fewer
+// triangle slots than kRaySortMinSlots are not sorted: their traversal is too cheap for the sort
+// to pay.
 constexpr int      kSortAxisBits    = 4;
-constexpr uint32_t kSortBuckets     = 8u << (3 * kSortAxisBits);
+constexpr uint32_t kSortCells       = 1u << (3 * kSortAxisBits);
+constexpr uint32_t kSortBuckets     = 8u * kSortCells;
 constexpr uint32_t kRaySortMinPaths = 1u << 18;
+constexpr uint32_t kRaySortMinSlots = 4096;
 
 struct Queues {
     uint32_t*       ext[2];
