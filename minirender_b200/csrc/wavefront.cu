@@ -676,31 +676,47 @@ __global__ void __launch_bounds__(128) shade_kernel(KernelArgs a) {
 
 // ---- coherence sort of the next bounce's extension rays ----
 
-// Exclusive scan of the bucket counts into the cursors, by one block of 1024 threads; the counts
-// are cleared for the next bounce.
+// Exclusive scan of the bucket counts into the cursors, by one block of 32 warps; the counts are
+// cleared for the next bounce. Warp w owns buckets [w * span, (w + 1) * span): a first pass sums
+// them (coalesced loads), one warp scans the 32 sums, and a second pass scans each range with its
+// base and writes the cursors.
 __global__ void __launch_bounds__(1024) sort_scan_kernel(uint32_t* buckets) {
-    constexpr uint32_t per = kSortBuckets / 1024;
-    __shared__ uint32_t partial[1024];
-    const uint32_t      t = threadIdx.x;
-    uint32_t            local[per];
-    uint32_t            sum = 0;
-    for (uint32_t k = 0; k < per; ++k) {
-        local[k]             = buckets[t * per + k];
-        buckets[t * per + k] = 0;
-        sum += local[k];
+    constexpr uint32_t span = kSortBuckets / 32;
+    __shared__ uint32_t warp_base[32];
+    const uint32_t      warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t*     counts = buckets + warp * span;
+    uint32_t            sum    = 0;
+    for (uint32_t k = lane; k < span; k += 32) {
+        sum += counts[k];
     }
-    partial[t] = sum;
+    sum = __reduce_add_sync(0xffffffffu, sum);
+    if (lane == 0) {
+        warp_base[warp] = sum;
+    }
     __syncthreads();
-    for (uint32_t offset = 1; offset < 1024; offset <<= 1) {
-        const uint32_t v = t >= offset ? partial[t - offset] : 0u;
-        __syncthreads();
-        partial[t] += v;
-        __syncthreads();
+    if (warp == 0) {
+        const uint32_t v = warp_base[lane];
+        uint32_t       x = v;
+        for (uint32_t offset = 1; offset < 32; offset <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, offset);
+            x += lane >= offset ? y : 0u;
+        }
+        warp_base[lane] = x - v;
     }
-    uint32_t run = partial[t] - sum;
-    for (uint32_t k = 0; k < per; ++k) {
-        buckets[kSortBuckets + t * per + k] = run;
-        run += local[k];
+    __syncthreads();
+    uint32_t  carry   = warp_base[warp];
+    uint32_t* mine    = buckets + warp * span;
+    uint32_t* cursors = buckets + kSortBuckets + warp * span;
+    for (uint32_t k = 0; k < span; k += 32) {
+        const uint32_t v = mine[k + lane];
+        uint32_t       x = v;
+        for (uint32_t offset = 1; offset < 32; offset <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, offset);
+            x += lane >= offset ? y : 0u;
+        }
+        cursors[k + lane] = carry + x - v;
+        mine[k + lane]    = 0;
+        carry += __shfl_sync(0xffffffffu, x, 31);
     }
 }
 
