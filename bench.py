@@ -755,32 +755,21 @@ def run_ours(args):
 
         phase = {"build": 0.0, "render": 0.0}
 
-        server = api.RenderServer(policy="shortest_first", batch=tuned) if jobs else None
-
         def e2e_step():
-            # Scenes are built on 8 host threads (construction runs on its own stream with
-            # stream-ordered buffers, so builds overlap one another on the GPU), and each job is
-            # submitted to the render server as soon as its scene exists: the first waves render
-            # while later scenes build. Every image is read back to host memory. With N ranks each
+            # Scenes are built on 8 host threads: construction runs on its own stream with
+            # stream-ordered buffers, so builds overlap one another on the GPU. (Submitting each
+            # job to the render server as its scene is ready was measured and is slower: the
+            # builder's kernels wait behind the persistent render kernels.) With N ranks each
             # renders its share and rank 0 gathers every image (the one collective).
-            from concurrent.futures import as_completed
             t0 = time.perf_counter()
-            fresh = [None] * len(snaps)
-            ids = [None] * len(snaps)
-            pending = {builders.submit(api.Scene, s, split_references=True): k
-                       for k, s in enumerate(snaps)}
-            for done in as_completed(pending):
-                k = pending[done]
-                fresh[k] = done.result()
-                ids[k] = server.submit(fresh[k], jobs[k].render, jobs[k].integrator)
+            fresh = list(builders.map(lambda s: api.Scene(s, split_references=True), snaps))
             t1 = time.perf_counter()
-            images = []
-            for k, jid in enumerate(ids):
-                server.wait(jid)
-                info = server.info(jid)
-                assert info["state"] == "completed", info
-                images.append(server.result(jid))
-                server.release(jid)
+            batch = [api.BatchJob(f, j.render, j.integrator) for f, j in zip(fresh, jobs)]
+            if batch:
+                images, codes, _ = api.render_batch(batch, tuned)
+                assert all(c == 0 for c in codes), codes
+            else:
+                images = []
             if world > 1:
                 gathered = [None] * world if rank == 0 else None
                 dist.gather_object(list(zip(mine, images)), gathered, dst=0)
@@ -805,8 +794,6 @@ def run_ours(args):
             dist.all_reduce(e2e_seconds, op=dist.ReduceOp.MAX)
         e2e_value = samples_total * args.steps / float(e2e_seconds.item()) / 1e6
         e2e_phase = phase
-        if server is not None:
-            server.close()
         if world > 1:  # every rank's bytes: the job's totals
             counts = torch.tensor([h2d, d2h], dtype=torch.float64, device="cuda")
             dist.all_reduce(counts)
@@ -904,11 +891,10 @@ def run_ours(args):
             "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h,
                     "step": "256 scene uploads from pinned memory + GPU BVH builds (8 host "
-                            "threads), each job submitted to the render server as its scene is "
-                            "ready (builds overlap the first waves) + image read-back "
-                            "(mr_scene_create_with + mr_server_submit / mr_server_result)",
-                    "submission_s_per_step": e2e_phase["build"] / args.steps if e2e_phase else None,
-                    "drain_s_per_step": e2e_phase["render"] / args.steps if e2e_phase else None},
+                            "threads) + batched render + image read-back "
+                            "(mr_scene_create_with + mr_render_batch)",
+                    "scene_build_s_per_step": e2e_phase["build"] / args.steps if e2e_phase else None,
+                    "render_s_per_step": e2e_phase["render"] / args.steps if e2e_phase else None},
             "gpu_launches": launches,
             "clocks": clock_info,
         }

@@ -59,6 +59,15 @@ void copy_path_radiance(Workspace& ws, uint32_t count, float* device_out, cudaSt
 
 namespace {
 
+// A non-blocking stream owned by one API call.
+struct CallStream {
+    cudaStream_t stream = nullptr;
+    CallStream() { MR_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking)); }
+    ~CallStream() { cudaStreamDestroy(stream); }
+    CallStream(const CallStream&)            = delete;
+    CallStream& operator=(const CallStream&) = delete;
+};
+
 thread_local std::string last_error;
 
 template <typename F> mr_status guarded(F&& f) {
@@ -699,11 +708,15 @@ mr_status mr_render_rows(const mr_scene* scene, const mr_integrator_settings* in
             }
             return;
         }
+        CallStream          call;
+        AllocationScope     scope(call.stream);
         DeviceBuffer<float> image;
         image.allocate(3 * pixels);
-        render_frame(s, p, *render, image.ptr, nullptr, statistics ? statistics : &local, 0,
+        render_frame(s, p, *render, image.ptr, call.stream, statistics ? statistics : &local, 0,
                      static_cast<uint32_t>(row_begin), static_cast<uint32_t>(row_end));
-        MR_CUDA(cudaMemcpy(rgb, image.ptr, 3 * pixels * sizeof(float), cudaMemcpyDeviceToHost));
+        MR_CUDA(cudaMemcpyAsync(rgb, image.ptr, 3 * pixels * sizeof(float), cudaMemcpyDeviceToHost,
+                                call.stream));
+        MR_CUDA(cudaStreamSynchronize(call.stream));
     });
 }
 
@@ -715,12 +728,17 @@ mr_status mr_render(const mr_scene* scene, const mr_integrator_settings* integra
         validate_render(render);
         require(rgb != nullptr, "Output image is null");
         const size_t        pixels = static_cast<size_t>(render->width) * render->height;
+        // The call's own stream and stream-ordered image buffer: no device-wide synchronisation
+        // from an allocation or from the legacy stream.
+        CallStream          call;
+        AllocationScope     scope(call.stream);
         DeviceBuffer<float> image;
         image.allocate(3 * pixels);
-        cudaStream_t       stream = nullptr;
         mr_path_statistics local{};
-        render_frame(s, p, *render, image.ptr, stream, statistics ? statistics : &local);
-        MR_CUDA(cudaMemcpy(rgb, image.ptr, 3 * pixels * sizeof(float), cudaMemcpyDeviceToHost));
+        render_frame(s, p, *render, image.ptr, call.stream, statistics ? statistics : &local);
+        MR_CUDA(cudaMemcpyAsync(rgb, image.ptr, 3 * pixels * sizeof(float), cudaMemcpyDeviceToHost,
+                                call.stream));
+        MR_CUDA(cudaStreamSynchronize(call.stream));
     });
 }
 
