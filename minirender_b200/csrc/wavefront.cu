@@ -618,7 +618,7 @@ __device__ ShadeResult shade_surface(const KernelArgs& a, uint32_t path, int bin
 }
 
 template <bool BATCH, bool TWO>
-__global__ void __launch_bounds__(128) shade_kernel(KernelArgs a) {
+__global__ void __launch_bounds__(128, 5) shade_kernel(KernelArgs a) {
     BounceCounters* ctr = a.q.counters + a.bounce;
     uint32_t        prefix[kBinCount + 1];
     prefix[0] = 0;

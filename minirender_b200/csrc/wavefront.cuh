@@ -140,14 +140,14 @@ struct PathState {
 };
 
 // Coherence sort of the extension rays between bounces: a counting sort on a key made of where
-// the ray starts (the position of its origin's triangle in the tree's leaf order, in 4,096 equal
-// ranges; or, for a medium vertex, the Morton code of its cell in the scene's bounds) and its
-// direction octant. Leaf order follows the tree, so a range covers a compact piece of geometry
+// the ray starts (the position of its origin's triangle in the tree's leaf order, in 16,384 equal
+// ranges; or, for a medium vertex, the Morton code of its cell in the scene's bounds, 4 bits per
+// axis) and its direction octant. Leaf order follows the tree, so a range covers a compact piece of geometry
 // however the geometry is spread. Waves of fewer paths than kRaySortMinPaths and scenes of fewer
 // triangle slots than kRaySortMinSlots are not sorted: their traversal is too cheap for the sort
 // to pay.
 constexpr int      kSortAxisBits    = 4;
-constexpr uint32_t kSortCells       = 1u << (3 * kSortAxisBits);
+constexpr uint32_t kSortCells       = 1u << 14;  // >= 2^(3 kSortAxisBits)
 constexpr uint32_t kSortBuckets     = 8u * kSortCells;
 constexpr uint32_t kRaySortMinPaths = 1u << 18;
 constexpr uint32_t kRaySortMinSlots = 4096;
