@@ -385,7 +385,8 @@ __global__ void __launch_bounds__(128, TWO ? 5 : 8) trace_kernel(KernelArgs a) {
 struct ShadeResult {
     bool     continue_path;
     bool     shadow;
-    uint32_t sort_key;  // coherence key of the continuing ray
+    uint32_t sort_key;         // coherence key of the continuing ray
+    uint32_t shadow_sort_key;  // and of the shadow ray
 };
 
 // Coherence key of a ray: where it starts, then its direction octant. A ray leaving a surface
@@ -459,7 +460,7 @@ __device__ ShadeResult shade_surface(const KernelArgs& a, uint32_t path, int bin
     const bool              previous_delta = a.st.flags[path] & 1u;
     float4                  L4    = a.st.radiance[path];
     f3                      L     = xyz(L4);
-    ShadeResult             out{false, false, 0u};
+    ShadeResult             out{false, false, 0u, 0u};
 
     if (bin == kBinMiss) {
         L += beta * environment_radiance(s, dir) *
@@ -499,6 +500,7 @@ __device__ ShadeResult shade_surface(const KernelArgs& a, uint32_t path, int bin
                 a.st.shadow_d[path] = f4(sd, 0);
                 a.st.shadow_c[path] = f4(beta * ls.radiance * (phase * weight / ls.probability), 0);
                 out.shadow          = true;
+                out.shadow_sort_key = a.q.staging ? coherence_key(s, kNone, vertex, sd) : 0u;
             }
         }
         float     pdf;
@@ -578,6 +580,7 @@ __device__ ShadeResult shade_surface(const KernelArgs& a, uint32_t path, int bin
                                                  (weight / ls.probability),
                                              0);
                     out.shadow = true;
+                    out.shadow_sort_key = a.q.staging ? coherence_key(s, slot, origin, sd) : 0u;
                 }
             }
         }
@@ -635,7 +638,7 @@ __global__ void __launch_bounds__(128, 5) shade_kernel(KernelArgs a) {
     for (uint32_t base = warp * 32; base < total; base += warps * 32) {
         const uint32_t i      = base + lane_id();
         uint32_t       path   = 0;
-        uint32_t       ext_key = kNone, shadow_key = kNone, sort_key = kNone;
+        uint32_t       ext_key = kNone, shadow_key = kNone, sort_key = kNone, shadow_sort = kNone;
         if (i < total) {
             int bin = 0;
             while (i >= prefix[bin + 1]) {
@@ -648,11 +651,23 @@ __global__ void __launch_bounds__(128, 5) shade_kernel(KernelArgs a) {
             ext_key              = r.continue_path ? 0u : kNone;
             shadow_key           = r.shadow ? 0u : kNone;
             sort_key             = r.continue_path ? r.sort_key : kNone;
+            shadow_sort          = r.shadow ? r.shadow_sort_key : kNone;
         }
-        warp_append(shadow_key, path, &ctr->shadow, a.q.shadow, 0);
         if (a.q.staging) {
-            // Staged for the coherence sort: the path at its position, its key beside it, and
-            // one count per distinct key per warp.
+            // Both queues are staged for the coherence sort: each entry's key beside it, one
+            // count per distinct key per warp (shadow keys in the second half of the counts).
+            const uint32_t pos = warp_append(shadow_key, path, &ctr->shadow, a.q.shadow_staging, 0);
+            if (shadow_key != kNone) {
+                a.q.shadow_keys[pos] = shadow_sort;
+            }
+            const unsigned same = __match_any_sync(0xffffffffu, shadow_sort);
+            if (shadow_sort != kNone && lane_id() == __ffs(same) - 1) {
+                atomicAdd(a.q.buckets + kSortBuckets + shadow_sort, static_cast<uint32_t>(__popc(same)));
+            }
+        } else {
+            warp_append(shadow_key, path, &ctr->shadow, a.q.shadow, 0);
+        }
+        if (a.q.staging) {
             const uint32_t pos = warp_append(ext_key, path, &nctr->ext, a.q.staging, 0);
             if (ext_key != kNone) {
                 a.q.keys[pos] = sort_key;
@@ -679,9 +694,10 @@ __global__ void __launch_bounds__(128, 5) shade_kernel(KernelArgs a) {
 // Exclusive scan of the bucket counts into the cursors, by one block of 32 warps; the counts are
 // cleared for the next bounce. Warp w owns buckets [w * span, (w + 1) * span): a first pass sums
 // them (coalesced loads), one warp scans the 32 sums, and a second pass scans each range with its
-// base and writes the cursors.
+// base and writes the cursors. Warps 0-15 hold the extension keys and 16-31 the shadow keys;
+// each half's cursors start at 0.
 __global__ void __launch_bounds__(1024) sort_scan_kernel(uint32_t* buckets) {
-    constexpr uint32_t span = kSortBuckets / 32;
+    constexpr uint32_t span = 2 * kSortBuckets / 32;
     __shared__ uint32_t warp_base[32];
     const uint32_t      warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t*     counts = buckets + warp * span;
@@ -701,12 +717,13 @@ __global__ void __launch_bounds__(1024) sort_scan_kernel(uint32_t* buckets) {
             const uint32_t y = __shfl_up_sync(0xffffffffu, x, offset);
             x += lane >= offset ? y : 0u;
         }
-        warp_base[lane] = x - v;
+        const uint32_t ext_total = __shfl_sync(0xffffffffu, x, 15);
+        warp_base[lane]          = x - v - (lane >= 16 ? ext_total : 0u);
     }
     __syncthreads();
     uint32_t  carry   = warp_base[warp];
     uint32_t* mine    = buckets + warp * span;
-    uint32_t* cursors = buckets + kSortBuckets + warp * span;
+    uint32_t* cursors = buckets + 2 * kSortBuckets + warp * span;
     for (uint32_t k = 0; k < span; k += 32) {
         const uint32_t v = mine[k + lane];
         uint32_t       x = v;
@@ -720,24 +737,35 @@ __global__ void __launch_bounds__(1024) sort_scan_kernel(uint32_t* buckets) {
     }
 }
 
-// Moves the staged paths into the next bounce's queue in key order (within a key, in the order
-// the warps claim their places: path results do not depend on queue order).
+// Moves the staged paths into the next bounce's extension queue and the staged shadow rays into
+// the shadow queue, each in key order (within a key, in the order the warps claim their places:
+// path results do not depend on queue order).
 __global__ void sort_scatter_kernel(KernelArgs a) {
-    const uint32_t n    = a.q.counters[a.bounce + 1].ext;
-    uint32_t*      next = a.q.ext[(a.bounce + 1) & 1];
-    const uint32_t step = gridDim.x * blockDim.x;
+    const uint32_t n_ext    = a.q.counters[a.bounce + 1].ext;
+    const uint32_t n_shadow = a.q.counters[a.bounce].shadow;
+    const uint32_t n        = n_ext + n_shadow;
+    uint32_t*      next     = a.q.ext[(a.bounce + 1) & 1];
+    const uint32_t step     = gridDim.x * blockDim.x;
     for (uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u; base < n; base += step) {
-        const uint32_t i    = base + lane_id();
-        const uint32_t key  = i < n ? a.q.keys[i] : kNone;
+        const uint32_t i      = base + lane_id();
+        const bool     shadow = i >= n_ext;
+        uint32_t       key    = kNone;
+        if (i < n) {
+            key = shadow ? kSortBuckets + a.q.shadow_keys[i - n_ext] : a.q.keys[i];
+        }
         const unsigned same = __match_any_sync(0xffffffffu, key);
         if (key != kNone) {
             const int leader = __ffs(same) - 1;
             uint32_t  pos    = 0;
             if (lane_id() == leader) {
-                pos = atomicAdd(a.q.buckets + kSortBuckets + key, static_cast<uint32_t>(__popc(same)));
+                pos = atomicAdd(a.q.buckets + 2 * kSortBuckets + key, static_cast<uint32_t>(__popc(same)));
             }
-            pos       = __shfl_sync(same, pos, leader) + __popc(same & ((1u << lane_id()) - 1u));
-            next[pos] = a.q.staging[i];
+            pos = __shfl_sync(same, pos, leader) + __popc(same & ((1u << lane_id()) - 1u));
+            if (shadow) {
+                a.q.shadow[pos] = a.q.shadow_staging[i - n_ext];
+            } else {
+                next[pos] = a.q.staging[i];
+            }
         }
     }
 }
@@ -938,7 +966,9 @@ std::shared_ptr<Workspace> allocate_workspace(size_t capacity, uint32_t max_boun
     const size_t o_shadow = field(capacity * sizeof(uint32_t));
     const size_t o_stage = field(capacity * sizeof(uint32_t));
     const size_t o_keys  = field(capacity * sizeof(uint32_t));
-    const size_t o_buck  = field(2 * kSortBuckets * sizeof(uint32_t));
+    const size_t o_sstage = field(capacity * sizeof(uint32_t));
+    const size_t o_skeys  = field(capacity * sizeof(uint32_t));
+    const size_t o_buck  = field(4 * kSortBuckets * sizeof(uint32_t));
     const size_t o_ctr = field((max_bounces + 2) * sizeof(BounceCounters));
     const size_t o_stats = field(kStatCount * sizeof(unsigned long long));
     const size_t o_err = field(sizeof(unsigned));
@@ -959,8 +989,10 @@ std::shared_ptr<Workspace> allocate_workspace(size_t capacity, uint32_t max_boun
     ws->queues.shadow       = reinterpret_cast<uint32_t*>(base + o_shadow);
     ws->queues.staging      = reinterpret_cast<uint32_t*>(base + o_stage);
     ws->queues.keys         = reinterpret_cast<uint32_t*>(base + o_keys);
+    ws->queues.shadow_staging = reinterpret_cast<uint32_t*>(base + o_sstage);
+    ws->queues.shadow_keys    = reinterpret_cast<uint32_t*>(base + o_skeys);
     ws->queues.buckets      = reinterpret_cast<uint32_t*>(base + o_buck);
-    MR_CUDA(cudaMemset(ws->queues.buckets, 0, kSortBuckets * sizeof(uint32_t)));  // counts start at 0
+    MR_CUDA(cudaMemset(ws->queues.buckets, 0, 2 * kSortBuckets * sizeof(uint32_t)));
     ws->queues.counters     = reinterpret_cast<BounceCounters*>(base + o_ctr);
     ws->queues.stats        = reinterpret_cast<unsigned long long*>(base + o_stats);
     ws->queues.error        = reinterpret_cast<unsigned*>(base + o_err);

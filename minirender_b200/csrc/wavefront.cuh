@@ -139,7 +139,7 @@ struct PathState {
     }
 };
 
-// Coherence sort of the extension rays between bounces: a counting sort on a key made of where
+// Coherence sort of the extension and shadow rays between bounces: a counting sort on a key made of where
 // the ray starts (the position of its origin's triangle in the tree's leaf order, in 16,384 equal
 // ranges; or, for a medium vertex, the Morton code of its cell in the scene's bounds, 4 bits per
 // axis) and its direction octant. Leaf order follows the tree, so a range covers a compact piece of geometry
@@ -156,7 +156,10 @@ struct Queues {
     uint32_t*       ext[2];
     uint32_t*       staging;  // this bounce's continuing paths before the sort (null: no sort)
     uint32_t*       keys;     // their sort keys, at the same positions
-    uint32_t*       buckets;  // kSortBuckets counts, then kSortBuckets cursors
+    uint32_t*       shadow_staging;  // this bounce's shadow rays before the sort
+    uint32_t*       shadow_keys;     // their sort keys
+    uint32_t*       buckets;  // 2 kSortBuckets counts (extension rays, then shadow rays), then the
+                              // 2 kSortBuckets cursors
     uint32_t*       bins;    // kBinCount * capacity
     uint32_t*       shadow;
     BounceCounters* counters;  // maximum_depth + 2 entries
