@@ -306,8 +306,9 @@ def run_reference(args):
     if rank != 0:
         return 0
     table = job_table(args.jobs)
-    budget = float(os.environ.get("BENCH_REFERENCE_SECONDS", 120.0))  # warmup + steps
-    sample = CpuSample(table, budget / max(1, args.steps + args.warmup))
+    # The same bounded sample as our arm's cpu_baseline (bands sized for --cpu-seconds), so the
+    # two CPU figures of a run measure the same rows; each step renders it once.
+    sample = CpuSample(table, args.cpu_seconds)
     for _ in range(args.warmup):
         sample.run()
     samples, seconds = 0, 0.0
