@@ -691,50 +691,89 @@ __global__ void __launch_bounds__(128, 5) shade_kernel(KernelArgs a) {
 
 // ---- coherence sort of the next bounce's extension rays ----
 
-// Exclusive scan of the bucket counts into the cursors, by one block of 32 warps; the counts are
-// cleared for the next bounce. Warp w owns buckets [w * span, (w + 1) * span): a first pass sums
-// them (coalesced loads), one warp scans the 32 sums, and a second pass scans each range with its
-// base and writes the cursors. Warps 0-15 hold the extension keys and 16-31 the shadow keys;
-// each half's cursors start at 0.
-__global__ void __launch_bounds__(1024) sort_scan_kernel(uint32_t* buckets) {
-    constexpr uint32_t span = 2 * kSortBuckets / 32;
-    __shared__ uint32_t warp_base[32];
-    const uint32_t      warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t*     counts = buckets + warp * span;
-    uint32_t            sum    = 0;
-    for (uint32_t k = lane; k < span; k += 32) {
-        sum += counts[k];
+// Exclusive scan of the bucket counts into the cursors, in three launches over blocks of 1,024
+// buckets (256 threads, 4 consecutive buckets each): block sums, a scan of the block sums, then
+// each block's scan from its base. The extension keys fill the first half of the buckets and the
+// shadow keys the second; each half's cursors start at 0. The counts are cleared for the next
+// bounce.
+constexpr uint32_t kSortScanBlock  = 1024;
+constexpr uint32_t kSortScanBlocks = 2 * kSortBuckets / kSortScanBlock;
+
+__device__ __forceinline__ uint32_t block_exclusive_scan_256(uint32_t v, uint32_t* warp_sums,
+                                                             uint32_t& total) {
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t       x    = v;
+    for (uint32_t offset = 1; offset < 32; offset <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, offset);
+        x += lane >= offset ? y : 0u;
     }
-    sum = __reduce_add_sync(0xffffffffu, sum);
-    if (lane == 0) {
-        warp_base[warp] = sum;
-    }
-    __syncthreads();
-    if (warp == 0) {
-        const uint32_t v = warp_base[lane];
-        uint32_t       x = v;
-        for (uint32_t offset = 1; offset < 32; offset <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, x, offset);
-            x += lane >= offset ? y : 0u;
-        }
-        const uint32_t ext_total = __shfl_sync(0xffffffffu, x, 15);
-        warp_base[lane]          = x - v - (lane >= 16 ? ext_total : 0u);
+    if (lane == 31) {
+        warp_sums[warp] = x;
     }
     __syncthreads();
-    uint32_t  carry   = warp_base[warp];
-    uint32_t* mine    = buckets + warp * span;
-    uint32_t* cursors = buckets + 2 * kSortBuckets + warp * span;
-    for (uint32_t k = 0; k < span; k += 32) {
-        const uint32_t v = mine[k + lane];
-        uint32_t       x = v;
-        for (uint32_t offset = 1; offset < 32; offset <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, x, offset);
-            x += lane >= offset ? y : 0u;
-        }
-        cursors[k + lane] = carry + x - v;
-        mine[k + lane]    = 0;
-        carry += __shfl_sync(0xffffffffu, x, 31);
+    uint32_t before = 0;
+    total           = 0;
+    for (uint32_t w = 0; w < 8; ++w) {
+        before += w < warp ? warp_sums[w] : 0u;
+        total += warp_sums[w];
     }
+    return before + x - v;
+}
+
+__global__ void __launch_bounds__(256) sort_block_sums_kernel(const uint32_t* buckets, uint32_t* sums) {
+    const uint4 c = reinterpret_cast<const uint4*>(buckets + blockIdx.x * kSortScanBlock)[threadIdx.x];
+    const uint32_t v = __reduce_add_sync(0xffffffffu, c.x + c.y + c.z + c.w);
+    __shared__ uint32_t warp_sums[8];
+    if ((threadIdx.x & 31) == 0) {
+        warp_sums[threadIdx.x >> 5] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = 0;
+        for (int w = 0; w < 8; ++w) {
+            t += warp_sums[w];
+        }
+        sums[blockIdx.x] = t;
+    }
+}
+
+__global__ void __launch_bounds__(256) sort_block_bases_kernel(uint32_t* sums) {
+    static_assert(kSortScanBlocks == 256, "one thread per block of buckets");
+    __shared__ uint32_t warp_sums[8];
+    const uint32_t      v = sums[threadIdx.x];
+    uint32_t            total;
+    uint32_t            base = block_exclusive_scan_256(v, warp_sums, total);
+    __syncthreads();
+    // The shadow half (blocks 128-255) starts again at 0.
+    __shared__ uint32_t extension_total;
+    if (threadIdx.x == kSortScanBlocks / 2) {
+        extension_total = base;
+    }
+    __syncthreads();
+    if (threadIdx.x >= kSortScanBlocks / 2) {
+        base -= extension_total;
+    }
+    sums[kSortScanBlocks + threadIdx.x] = base;
+}
+
+__global__ void __launch_bounds__(256) sort_cursors_kernel(uint32_t* buckets, const uint32_t* sums) {
+    __shared__ uint32_t warp_sums[8];
+    uint4*         counts = reinterpret_cast<uint4*>(buckets + blockIdx.x * kSortScanBlock);
+    uint4*         cursors =
+        reinterpret_cast<uint4*>(buckets + 2 * kSortBuckets + blockIdx.x * kSortScanBlock);
+    const uint4    c = counts[threadIdx.x];
+    uint32_t       total;
+    const uint32_t start = sums[kSortScanBlocks + blockIdx.x] +
+                           block_exclusive_scan_256(c.x + c.y + c.z + c.w, warp_sums, total);
+    cursors[threadIdx.x] = make_uint4(start, start + c.x, start + c.x + c.y, start + c.x + c.y + c.z);
+    counts[threadIdx.x]  = make_uint4(0, 0, 0, 0);
+}
+
+__host__ void enqueue_sort_scan(uint32_t* buckets, cudaStream_t stream) {
+    uint32_t* sums = buckets + 4 * kSortBuckets;
+    sort_block_sums_kernel<<<kSortScanBlocks, 256, 0, stream>>>(buckets, sums);
+    sort_block_bases_kernel<<<1, 256, 0, stream>>>(sums);
+    sort_cursors_kernel<<<kSortScanBlocks, 256, 0, stream>>>(buckets, sums);
 }
 
 // Moves the staged paths into the next bounce's extension queue and the staged shadow rays into
@@ -968,7 +1007,7 @@ std::shared_ptr<Workspace> allocate_workspace(size_t capacity, uint32_t max_boun
     const size_t o_keys  = field(capacity * sizeof(uint32_t));
     const size_t o_sstage = field(capacity * sizeof(uint32_t));
     const size_t o_skeys  = field(capacity * sizeof(uint32_t));
-    const size_t o_buck  = field(4 * kSortBuckets * sizeof(uint32_t));
+    const size_t o_buck  = field((4 * kSortBuckets + 2 * kSortScanBlocks) * sizeof(uint32_t));
     const size_t o_ctr = field((max_bounces + 2) * sizeof(BounceCounters));
     const size_t o_stats = field(kStatCount * sizeof(unsigned long long));
     const size_t o_err = field(sizeof(unsigned));
@@ -1150,7 +1189,7 @@ void Engine::run_wave(const Scene& scene, const IntegratorParams& params, const 
     KernelTiming&      timing = kernel_timing();
     bool               timed  = false;
     timed = timing.enabled.load();
-    note_launches(1 + 2ull * (params.maximum_depth + 1) + (ray_sort ? 2ull * params.maximum_depth : 0ull) +
+    note_launches(1 + 2ull * (params.maximum_depth + 1) + (ray_sort ? 4ull * params.maximum_depth : 0ull) +
                   (init.capture ? 1 : 0));
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
     // The timed launches are the trace kernels: nearest-hit and shadow tests both count.
@@ -1188,7 +1227,7 @@ void Engine::run_wave(const Scene& scene, const IntegratorParams& params, const 
             shade_kernel<false, false><<<shape.shade_blocks, 128, 0, stream>>>(a);
         }
         if (ray_sort && bounce < params.maximum_depth) {
-            sort_scan_kernel<<<1, 1024, 0, stream>>>(a.q.buckets);
+            enqueue_sort_scan(a.q.buckets, stream);
             sort_scatter_kernel<<<shape.shade_blocks, 128, 0, stream>>>(a);
         }
         if (bounce == 0 && init.capture) {
@@ -1273,7 +1312,7 @@ void Engine::enqueue_batch_paths(const WaveDesc* wave, uint32_t maximum_depth, b
             shade_kernel<true, false><<<shape.shade_blocks, 128, 0, stream>>>(a);
         }
         if (ray_sort && bounce < maximum_depth) {
-            sort_scan_kernel<<<1, 1024, 0, stream>>>(a.q.buckets);
+            enqueue_sort_scan(a.q.buckets, stream);
             sort_scatter_kernel<<<shape.shade_blocks, 128, 0, stream>>>(a);
         }
     }

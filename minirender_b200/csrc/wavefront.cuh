@@ -239,7 +239,7 @@ class Engine {
 
     // Kernel launches of one wave (paths + resolve).
     static uint64_t batch_wave_launches(uint32_t maximum_depth, bool ray_sort) {
-        return 2ull + 2ull * (maximum_depth + 1) + (ray_sort ? 2ull * maximum_depth : 0ull);
+        return 2ull + 2ull * (maximum_depth + 1) + (ray_sort ? 4ull * maximum_depth : 0ull);
     }
 };
 
