@@ -1,13 +1,18 @@
 // wavefront.cu — wavefront path tracing on the GPU.
 //
-// One wave = up to `capacity` camera paths. Each bounce runs three persistent kernels:
-//   extend  nearest-hit traversal of the bounce's ray queue; classifies every path into a
+// One wave = up to `capacity` camera paths, their state in one 128-byte record per path. Each
+// bounce runs two persistent kernels:
+//   trace   nearest-hit traversal of the bounce's ray queue, classifying every path into a
 //           material bin (miss, diffuse, conductor, mirror, dielectric, medium) with
-//           warp-aggregated appends (match_any + popc + one atomic per key per warp);
+//           warp-aggregated appends (match_any + popc + one atomic per key per warp), then
+//           any-hit traversal of the previous bounce's shadow queue, adding the unoccluded
+//           contributions;
 //   shade   emission with MIS, next-event estimation, BSDF sampling and Russian roulette,
 //           processed bin by bin so warps execute one material's code; appends the shadow
-//           queue and the next bounce's ray queue;
-//   shadow  any-hit traversal of the shadow queue, adding the unoccluded contributions.
+//           queue and the next bounce's ray queue.
+// In large waves of non-trivial scenes both queues are then sorted by where each ray starts and
+// its direction octant (a counting sort: keys counted in the shading launch, a scan, a scatter),
+// so that neighbouring lanes of the next traversal walk the same nodes.
 // The per-path logic is PathTracer::trace (src/render/path_tracer.cpp:153-366) in FP32 with the
 // reference's RNG stream layout; every path writes only its own state, so images do not depend
 // on scheduling. Radiance is kept per path and added to the pixels in sample order after the
