@@ -1334,19 +1334,44 @@ void Engine::enqueue_batch_resolve(const WaveDesc* wave, Workspace& ws, cudaStre
 
 void render_tile(const Scene& scene, const IntegratorParams& params, const mr_render_settings& render,
                  uint32_t x0, uint32_t y0, uint32_t w, uint32_t h, uint32_t s0, uint32_t ns,
-                 float4* accumulator, Workspace& ws, cudaStream_t stream, uint32_t accumulator_row0) {
+                 float4* accumulator, Workspace& ws, cudaStream_t stream, uint32_t accumulator_row0,
+                 Workspace* ws2, cudaStream_t stream2) {
     const size_t area = static_cast<size_t>(w) * h;
     if (area == 0 || ns == 0) {
         return;
     }
+    // Events of the two-lane mode: the lanes' start, the last resolve of each lane, the end.
+    struct Events {
+        cudaEvent_t e[4] = {nullptr, nullptr, nullptr, nullptr};
+        ~Events() {
+            for (cudaEvent_t x : e) {
+                if (x) {
+                    cudaEventDestroy(x);
+                }
+            }
+        }
+    } events;
+    const bool two = ws2 != nullptr && stream2 != nullptr;
+    if (two) {
+        for (cudaEvent_t& x : events.e) {
+            MR_CUDA(cudaEventCreateWithFlags(&x, cudaEventDisableTiming));
+        }
+        MR_CUDA(cudaEventRecord(events.e[0], stream));  // the accumulator is ready
+        MR_CUDA(cudaStreamWaitEvent(stream2, events.e[0], 0));
+    }
     // Split the sample range (and, for huge tiles, the rows) into waves that fit the workspace.
+    const size_t   capacity = two ? std::min(ws.capacity, ws2->capacity) : ws.capacity;
     const uint32_t rows_per_wave =
-        area <= ws.capacity ? h : static_cast<uint32_t>(std::max<size_t>(1, ws.capacity / w));
+        area <= capacity ? h : static_cast<uint32_t>(std::max<size_t>(1, capacity / w));
+    uint32_t wave = 0;
     for (uint32_t ry = 0; ry < h; ry += rows_per_wave) {
         const uint32_t hh      = std::min(rows_per_wave, h - ry);
         const size_t   a       = static_cast<size_t>(w) * hh;
-        const uint32_t per     = static_cast<uint32_t>(std::max<size_t>(1, std::min<size_t>(ns, ws.capacity / a)));
-        for (uint32_t s = 0; s < ns; s += per) {
+        const uint32_t per     = static_cast<uint32_t>(std::max<size_t>(1, std::min<size_t>(ns, capacity / a)));
+        for (uint32_t s = 0; s < ns; s += per, ++wave) {
+            const bool         second = two && (wave & 1u);
+            Workspace&         lane   = second ? *ws2 : ws;
+            const cudaStream_t ls     = second ? stream2 : stream;
             WaveInit init{};
             init.kind   = kInitCamera;
             init.x0     = x0;
@@ -1359,12 +1384,22 @@ void render_tile(const Scene& scene, const IntegratorParams& params, const mr_re
             init.height = static_cast<uint32_t>(render.height);
             init.seed   = render.seed;
             init.count  = static_cast<uint32_t>(a * init.ns);
-            Engine::run_wave(scene, params, init, ws, stream);
+            Engine::run_wave(scene, params, init, lane, ls);
+            if (two && wave > 0) {  // after the previous wave's resolve, on the other lane
+                MR_CUDA(cudaStreamWaitEvent(ls, events.e[second ? 1 : 2], 0));
+            }
             note_launches(1);
-            resolve_kernel<<<static_cast<unsigned>((a + 255) / 256), 256, 0, stream>>>(
-                ws.state.radiance, init.x0, init.y0, w, hh, init.ns, init.width, accumulator,
-                accumulator_row0, ws.queues.error);
+            resolve_kernel<<<static_cast<unsigned>((a + 255) / 256), 256, 0, ls>>>(
+                lane.state.radiance, init.x0, init.y0, w, hh, init.ns, init.width, accumulator,
+                accumulator_row0, lane.queues.error);
+            if (two) {
+                MR_CUDA(cudaEventRecord(events.e[second ? 2 : 1], ls));
+            }
         }
+    }
+    if (two) {
+        MR_CUDA(cudaEventRecord(events.e[3], stream2));
+        MR_CUDA(cudaStreamWaitEvent(stream, events.e[3], 0));
     }
     MR_CUDA(cudaGetLastError());
 }
@@ -1384,16 +1419,50 @@ void render_frame(const Scene& scene, const IntegratorParams& params, const mr_r
     }
     const size_t capacity = std::min(total, max_paths ? max_paths : (size_t(1) << 23));
     auto         ws       = acquire_workspace(capacity, params.maximum_depth + 1, pixels);
+    // A frame of several waves alternates them between two workspaces on two streams.
+    struct SecondLane {
+        std::shared_ptr<Workspace> ws;
+        cudaStream_t               stream = nullptr;
+        ~SecondLane() {
+            if (stream) {
+                cudaStreamDestroy(stream);
+            }
+            if (ws) {
+                release_workspace(ws);
+            }
+        }
+    } second;
+    if (total > capacity && max_paths == 0) {
+        second.ws = acquire_workspace(capacity, params.maximum_depth + 1, 0);
+        MR_CUDA(cudaStreamCreateWithFlags(&second.stream, cudaStreamNonBlocking));
+        reset_statistics(*second.ws, stream);
+    }
     reset_statistics(*ws, stream);
     MR_CUDA(cudaMemsetAsync(ws->accumulator, 0, 2 * pixels * sizeof(float4), stream));
     render_tile(scene, params, render, 0, row_begin, static_cast<uint32_t>(render.width), rows, 0,
-                render.samples_per_pixel, ws->accumulator, *ws, stream, row_begin);
+                render.samples_per_pixel, ws->accumulator, *ws, stream, row_begin, second.ws.get(),
+                second.stream);
     note_launches(1);
     finalize_kernel<<<static_cast<unsigned>((pixels + 255) / 256), 256, 0, stream>>>(
         ws->accumulator, pixels, render.samples_per_pixel, device_rgb, ws->queues.error);
     MR_CUDA(cudaGetLastError());
     unsigned error = 0;
     read_statistics(*ws, stream, statistics, &error);
+    if (second.ws) {
+        mr_path_statistics more{};
+        unsigned           more_error = 0;
+        read_statistics(*second.ws, stream, statistics ? &more : nullptr, &more_error);
+        error |= more_error;
+        if (statistics) {
+            statistics->paths += more.paths;
+            statistics->shadow_rays += more.shadow_rays;
+            statistics->scattering_events += more.scattering_events;
+            statistics->roulette_terminations += more.roulette_terminations;
+            statistics->medium_scattering_events += more.medium_scattering_events;
+            statistics->geometry.bounds_tests += more.geometry.bounds_tests;
+            statistics->geometry.triangle_tests += more.geometry.triangle_tests;
+        }
+    }
     release_workspace(ws);
     std::string message;
     const mr_status status = error_status(error, message);

@@ -276,10 +276,14 @@ void render_frame(const Scene& scene, const IntegratorParams& params, const mr_r
 
 // Accumulates the samples [s0, s0+ns) of a pixel rectangle into a caller-owned Kahan
 // accumulator (float4 sum + float4 compensation per pixel of the full image).
-// The accumulator's first row is image row `accumulator_row0`.
+// The accumulator's first row is image row `accumulator_row0`. With a second workspace and
+// stream (`ws2`, `stream2`) consecutive waves alternate between the two, so one wave's last,
+// sparse bounces overlap the next wave's first; the resolves still run one after the other in
+// wave order (per pixel, samples accumulate in order), and `stream` waits for all of it.
 void render_tile(const Scene& scene, const IntegratorParams& params, const mr_render_settings& render,
                  uint32_t x0, uint32_t y0, uint32_t w, uint32_t h, uint32_t s0, uint32_t ns,
-                 float4* accumulator, Workspace& ws, cudaStream_t stream, uint32_t accumulator_row0 = 0);
+                 float4* accumulator, Workspace& ws, cudaStream_t stream, uint32_t accumulator_row0 = 0,
+                 Workspace* ws2 = nullptr, cudaStream_t stream2 = nullptr);
 
 void read_statistics(Workspace& ws, cudaStream_t stream, mr_path_statistics* out, unsigned* error);
 void reset_statistics(Workspace& ws, cudaStream_t stream);
