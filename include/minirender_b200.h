@@ -479,7 +479,10 @@ mr_status mr_display_image(const float* linear, uint64_t width, uint64_t height,
  * every launch of the nearest-hit traversal kernel on its launching stream; `mr_kernel_timing`
  * returns the number of those launches, their summed device time in seconds, the summed
  * bounds/triangle test counters of those launches, and the number of all kernels the library
- * launched while timing was enabled. Enabling resets the figures. No reference counterpart. */
+ * launched while timing was enabled. Enabling resets the figures. While it is enabled each wave
+ * of a plain render waits for the host to read its events, so the waves of a frame no longer
+ * overlap on the frame's lanes: time the render itself with timing disabled. No reference
+ * counterpart. */
 mr_status mr_set_kernel_timing(int enabled);
 mr_status mr_kernel_timing(uint64_t* launches, double* seconds, mr_trace_statistics* counted,
                            uint64_t* all_launches);

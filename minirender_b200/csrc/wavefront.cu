@@ -1335,32 +1335,55 @@ void Engine::enqueue_batch_resolve(const WaveDesc* wave, Workspace& ws, cudaStre
 void render_tile(const Scene& scene, const IntegratorParams& params, const mr_render_settings& render,
                  uint32_t x0, uint32_t y0, uint32_t w, uint32_t h, uint32_t s0, uint32_t ns,
                  float4* accumulator, Workspace& ws, cudaStream_t stream, uint32_t accumulator_row0,
-                 Workspace* ws2, cudaStream_t stream2) {
+                 const TileLane* more, uint32_t more_count) {
     const size_t area = static_cast<size_t>(w) * h;
     if (area == 0 || ns == 0) {
         return;
     }
-    // Events of the two-lane mode: the lanes' start, the last resolve of each lane, the end.
+    constexpr uint32_t kMaxLanes = 4;
+    TileLane           lanes[kMaxLanes];
+    uint32_t           lane_count = 1;
+    lanes[0]                      = TileLane{&ws, stream};
+    for (uint32_t i = 0; i < more_count && lane_count < kMaxLanes; ++i) {
+        if (more[i].ws && more[i].stream) {
+            lanes[lane_count++] = more[i];
+        }
+    }
+    // Events of the multi-lane mode: the start, each lane's last resolve, each lane's end.
     struct Events {
-        cudaEvent_t e[4] = {nullptr, nullptr, nullptr, nullptr};
+        cudaEvent_t start = nullptr;
+        cudaEvent_t resolved[kMaxLanes] = {};
+        cudaEvent_t done[kMaxLanes]     = {};
         ~Events() {
-            for (cudaEvent_t x : e) {
+            for (cudaEvent_t x : resolved) {
                 if (x) {
                     cudaEventDestroy(x);
                 }
             }
+            for (cudaEvent_t x : done) {
+                if (x) {
+                    cudaEventDestroy(x);
+                }
+            }
+            if (start) {
+                cudaEventDestroy(start);
+            }
         }
     } events;
-    const bool two = ws2 != nullptr && stream2 != nullptr;
-    if (two) {
-        for (cudaEvent_t& x : events.e) {
-            MR_CUDA(cudaEventCreateWithFlags(&x, cudaEventDisableTiming));
+    size_t capacity = ws.capacity;
+    if (lane_count > 1) {
+        MR_CUDA(cudaEventCreateWithFlags(&events.start, cudaEventDisableTiming));
+        MR_CUDA(cudaEventRecord(events.start, stream));  // the accumulator is ready
+        for (uint32_t i = 0; i < lane_count; ++i) {
+            MR_CUDA(cudaEventCreateWithFlags(&events.resolved[i], cudaEventDisableTiming));
+            MR_CUDA(cudaEventCreateWithFlags(&events.done[i], cudaEventDisableTiming));
+            capacity = std::min(capacity, lanes[i].ws->capacity);
+            if (i > 0) {
+                MR_CUDA(cudaStreamWaitEvent(lanes[i].stream, events.start, 0));
+            }
         }
-        MR_CUDA(cudaEventRecord(events.e[0], stream));  // the accumulator is ready
-        MR_CUDA(cudaStreamWaitEvent(stream2, events.e[0], 0));
     }
     // Split the sample range (and, for huge tiles, the rows) into waves that fit the workspace.
-    const size_t   capacity = two ? std::min(ws.capacity, ws2->capacity) : ws.capacity;
     const uint32_t rows_per_wave =
         area <= capacity ? h : static_cast<uint32_t>(std::max<size_t>(1, capacity / w));
     uint32_t wave = 0;
@@ -1369,9 +1392,9 @@ void render_tile(const Scene& scene, const IntegratorParams& params, const mr_re
         const size_t   a       = static_cast<size_t>(w) * hh;
         const uint32_t per     = static_cast<uint32_t>(std::max<size_t>(1, std::min<size_t>(ns, capacity / a)));
         for (uint32_t s = 0; s < ns; s += per, ++wave) {
-            const bool         second = two && (wave & 1u);
-            Workspace&         lane   = second ? *ws2 : ws;
-            const cudaStream_t ls     = second ? stream2 : stream;
+            const uint32_t     li   = wave % lane_count;
+            Workspace&         lane = *lanes[li].ws;
+            const cudaStream_t ls   = lanes[li].stream;
             WaveInit init{};
             init.kind   = kInitCamera;
             init.x0     = x0;
@@ -1385,21 +1408,21 @@ void render_tile(const Scene& scene, const IntegratorParams& params, const mr_re
             init.seed   = render.seed;
             init.count  = static_cast<uint32_t>(a * init.ns);
             Engine::run_wave(scene, params, init, lane, ls);
-            if (two && wave > 0) {  // after the previous wave's resolve, on the other lane
-                MR_CUDA(cudaStreamWaitEvent(ls, events.e[second ? 1 : 2], 0));
+            if (lane_count > 1 && wave > 0) {  // after the previous wave's resolve, on its lane
+                MR_CUDA(cudaStreamWaitEvent(ls, events.resolved[(wave - 1) % lane_count], 0));
             }
             note_launches(1);
             resolve_kernel<<<static_cast<unsigned>((a + 255) / 256), 256, 0, ls>>>(
                 lane.state.radiance, init.x0, init.y0, w, hh, init.ns, init.width, accumulator,
                 accumulator_row0, lane.queues.error);
-            if (two) {
-                MR_CUDA(cudaEventRecord(events.e[second ? 2 : 1], ls));
+            if (lane_count > 1) {
+                MR_CUDA(cudaEventRecord(events.resolved[li], ls));
             }
         }
     }
-    if (two) {
-        MR_CUDA(cudaEventRecord(events.e[3], stream2));
-        MR_CUDA(cudaStreamWaitEvent(stream, events.e[3], 0));
+    for (uint32_t i = 1; i < lane_count; ++i) {
+        MR_CUDA(cudaEventRecord(events.done[i], lanes[i].stream));
+        MR_CUDA(cudaStreamWaitEvent(stream, events.done[i], 0));
     }
     MR_CUDA(cudaGetLastError());
 }
@@ -1419,50 +1442,61 @@ void render_frame(const Scene& scene, const IntegratorParams& params, const mr_r
     }
     const size_t capacity = std::min(total, max_paths ? max_paths : (size_t(1) << 23));
     auto         ws       = acquire_workspace(capacity, params.maximum_depth + 1, pixels);
-    // A frame of several waves alternates them between two workspaces on two streams.
-    struct SecondLane {
-        std::shared_ptr<Workspace> ws;
-        cudaStream_t               stream = nullptr;
-        ~SecondLane() {
-            if (stream) {
-                cudaStreamDestroy(stream);
-            }
-            if (ws) {
-                release_workspace(ws);
+    // A frame of several waves goes round kFrameLanes workspaces, each with its own stream.
+    // The extra workspaces go back to the pool only once the frame has finished; after an error
+    // they are freed (cudaFree waits for the work still queued on them).
+    struct MoreLanes {
+        std::shared_ptr<Workspace> ws[kFrameLanes - 1];
+        TileLane                   lanes[kFrameLanes - 1];
+        uint32_t                   count    = 0;
+        bool                       finished = false;
+        ~MoreLanes() {
+            for (uint32_t i = 0; i < count; ++i) {
+                if (lanes[i].stream) {
+                    cudaStreamDestroy(lanes[i].stream);
+                }
+                if (finished) {
+                    release_workspace(ws[i]);
+                }
             }
         }
-    } second;
+    } more;
     if (total > capacity && max_paths == 0) {
-        second.ws = acquire_workspace(capacity, params.maximum_depth + 1, 0);
-        MR_CUDA(cudaStreamCreateWithFlags(&second.stream, cudaStreamNonBlocking));
-        reset_statistics(*second.ws, stream);
+        const size_t waves = (total + capacity - 1) / capacity;
+        for (uint32_t i = 0; i + 1 < kFrameLanes && i + 1 < waves; ++i) {
+            more.ws[i]       = acquire_workspace(capacity, params.maximum_depth + 1, 0);
+            more.lanes[i].ws = more.ws[i].get();
+            ++more.count;
+            MR_CUDA(cudaStreamCreateWithFlags(&more.lanes[i].stream, cudaStreamNonBlocking));
+            reset_statistics(*more.ws[i], stream);
+        }
     }
     reset_statistics(*ws, stream);
     MR_CUDA(cudaMemsetAsync(ws->accumulator, 0, 2 * pixels * sizeof(float4), stream));
     render_tile(scene, params, render, 0, row_begin, static_cast<uint32_t>(render.width), rows, 0,
-                render.samples_per_pixel, ws->accumulator, *ws, stream, row_begin, second.ws.get(),
-                second.stream);
+                render.samples_per_pixel, ws->accumulator, *ws, stream, row_begin, more.lanes, more.count);
     note_launches(1);
     finalize_kernel<<<static_cast<unsigned>((pixels + 255) / 256), 256, 0, stream>>>(
         ws->accumulator, pixels, render.samples_per_pixel, device_rgb, ws->queues.error);
     MR_CUDA(cudaGetLastError());
     unsigned error = 0;
     read_statistics(*ws, stream, statistics, &error);
-    if (second.ws) {
-        mr_path_statistics more{};
-        unsigned           more_error = 0;
-        read_statistics(*second.ws, stream, statistics ? &more : nullptr, &more_error);
-        error |= more_error;
+    for (uint32_t i = 0; i < more.count; ++i) {
+        mr_path_statistics other{};
+        unsigned           other_error = 0;
+        read_statistics(*more.ws[i], stream, statistics ? &other : nullptr, &other_error);
+        error |= other_error;
         if (statistics) {
-            statistics->paths += more.paths;
-            statistics->shadow_rays += more.shadow_rays;
-            statistics->scattering_events += more.scattering_events;
-            statistics->roulette_terminations += more.roulette_terminations;
-            statistics->medium_scattering_events += more.medium_scattering_events;
-            statistics->geometry.bounds_tests += more.geometry.bounds_tests;
-            statistics->geometry.triangle_tests += more.geometry.triangle_tests;
+            statistics->paths += other.paths;
+            statistics->shadow_rays += other.shadow_rays;
+            statistics->scattering_events += other.scattering_events;
+            statistics->roulette_terminations += other.roulette_terminations;
+            statistics->medium_scattering_events += other.medium_scattering_events;
+            statistics->geometry.bounds_tests += other.geometry.bounds_tests;
+            statistics->geometry.triangle_tests += other.geometry.triangle_tests;
         }
     }
+    more.finished = true;
     release_workspace(ws);
     std::string message;
     const mr_status status = error_status(error, message);

@@ -1,11 +1,13 @@
-"""A frame larger than one wave (8,388,608 paths) alternates its waves between two workspaces on
-two streams, so that one wave's last, sparse bounces overlap the next wave's first. The resolves
-still accumulate the waves in sample order: the image is bit for bit the single-lane render's.
+"""A frame larger than one wave (8,388,608 paths) sends its waves round three workspaces, each
+with its own stream, so that one wave's last, sparse bounces overlap the next waves' first. The
+resolves still accumulate the waves in sample order: the image is bit for bit the single-lane
+render's.
 
-A 1024x768 frame at 24 samples per pixel takes three waves of 10, 10 and 4 samples (lanes A, B,
-A); it is compared with a session that accumulates the same frame two samples per pixel per wave
-on one lane. A 1280x720 frame at 20 samples per pixel (three waves) is compared with three row
-ranges of one wave each, and its statistics (the sum of both workspaces' counters) with theirs.
+A 1024x768 frame at 24 samples per pixel takes three waves of 10, 10 and 4 samples (one per
+lane); it is compared with a session that accumulates the same frame two samples per pixel per
+wave on one lane. A 1280x720 frame at 40 samples per pixel takes five waves (the first two lanes
+take a second wave each); it is compared with five row ranges of one wave each, and its
+statistics (the sum of all lanes' counters) with theirs.
 """
 
 import numpy as np
@@ -22,7 +24,7 @@ def api():
     return a
 
 
-def test_two_lane_frame_equals_single_lane_session(api):
+def test_three_lane_frame_equals_single_lane_session(api):
     scene = api.Scene(sc.job_scene(60_000, 12).snapshot(), split_references=True)
     settings = api.IntegratorSettings("mis", 8, True, 3)
     render = api.RenderSettings(1024, 768, 24, 5)
@@ -38,13 +40,13 @@ def test_two_lane_frame_equals_single_lane_session(api):
     assert image.mean() > 0 and stats["shadow_rays"] > 0
 
 
-def test_two_lane_frame_equals_single_wave_row_ranges(api):
+def test_five_wave_frame_equals_single_wave_row_ranges(api):
     scene = api.Scene(sc.job_scene(30_000, 4).snapshot())
     tracer = api.PathTracer(scene, api.IntegratorSettings("mis", 6, True, 3))
-    render = api.RenderSettings(1280, 720, 20, 8)  # 18,432,000 paths: three waves
+    render = api.RenderSettings(1280, 720, 40, 8)  # 36,864,000 paths: five waves
     image, stats = tracer.render(render)
     total = dict.fromkeys(("paths", "shadow_rays", "scattering_events", "roulette_terminations"), 0)
-    for r0, r1 in ((0, 300), (300, 600), (600, 720)):  # at most 7,680,000 paths: one wave each
+    for r0, r1 in ((0, 150), (150, 300), (300, 450), (450, 600), (600, 720)):  # one wave each
         rows, part = tracer.render_rows(render, r0, r1, statistics=True)
         np.testing.assert_array_equal(rows, image[r0:r1])
         for key in total:
