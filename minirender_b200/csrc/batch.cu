@@ -1150,7 +1150,7 @@ mr_status mr_batch_autotune(const mr_batch_job* jobs, size_t count, mr_batch_set
         int trace_max = 0, shade_max = 0;
         Engine::batch_occupancy(trace_max, shade_max);
         const uint64_t waves[]      = {size_t(1) << 21, size_t(1) << 22, size_t(1) << 23};
-        const uint32_t lanes[]      = {1u, 2u, 3u};
+        const uint32_t lanes[]      = {1u, 2u, 3u, 4u};
         const uint32_t thresholds[] = {0u, 1u << 15};
         // Samples per device second of one calibration render (the engine's own events, so the
         // host-side setup of a new wave shape is not counted).
