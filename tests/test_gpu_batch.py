@@ -171,7 +171,7 @@ def test_failing_job_fails_alone(api, scenes):
 def test_autotune_returns_a_valid_shape(api, scenes):
     jobs = job_mix(api, scenes)[:2]
     best, rate = api.autotune(jobs)
-    assert best.wave_paths in (1 << 21, 1 << 22, 1 << 23) and 1 <= best.concurrent_waves <= 3
+    assert best.wave_paths in (1 << 21, 1 << 22, 1 << 23) and 1 <= best.concurrent_waves <= 4
     assert rate > 0
     images, codes, _ = api.render_batch(jobs, best)
     assert codes == [0, 0]
