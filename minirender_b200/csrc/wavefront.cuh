@@ -153,8 +153,8 @@ constexpr uint32_t kRaySortMinPaths = 1u << 18;
 constexpr uint32_t kRaySortMinSlots = 4096;
 // Lanes (workspace + stream) that a plain frame of several waves goes round, so that one wave's
 // last bounces overlap the next waves' first (two lanes: 1M-triangle frame -7.0%; three: a
-// further -1.7%).
-constexpr uint32_t kFrameLanes = 3;
+// further -1.7%; four: a further -1.0%).
+constexpr uint32_t kFrameLanes = 4;
 
 struct Queues {
     uint32_t*       ext[2];

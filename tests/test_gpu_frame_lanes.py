@@ -1,13 +1,13 @@
-"""A frame larger than one wave (8,388,608 paths) sends its waves round three workspaces, each
+"""A frame larger than one wave (8,388,608 paths) sends its waves round four workspaces, each
 with its own stream, so that one wave's last, sparse bounces overlap the next waves' first. The
 resolves still accumulate the waves in sample order: the image is bit for bit the single-lane
 render's.
 
-A 1024x768 frame at 24 samples per pixel takes three waves of 10, 10 and 4 samples (one per
-lane); it is compared with a session that accumulates the same frame two samples per pixel per
-wave on one lane. A 1280x720 frame at 40 samples per pixel takes five waves (the first two lanes
-take a second wave each); it is compared with five row ranges of one wave each, and its
-statistics (the sum of all lanes' counters) with theirs.
+A 1024x768 frame at 24 samples per pixel takes three waves of 10, 10 and 4 samples (one lane
+each); it is compared with a session that accumulates the same frame two samples per pixel per
+wave on one lane. A 1280x720 frame at 40 samples per pixel takes five waves (the first lane takes
+a second one); it is compared with five row ranges of one wave each, and its statistics (the sum
+of all lanes' counters) with theirs.
 """
 
 import numpy as np
@@ -24,7 +24,7 @@ def api():
     return a
 
 
-def test_three_lane_frame_equals_single_lane_session(api):
+def test_multi_lane_frame_equals_single_lane_session(api):
     scene = api.Scene(sc.job_scene(60_000, 12).snapshot(), split_references=True)
     settings = api.IntegratorSettings("mis", 8, True, 3)
     render = api.RenderSettings(1024, 768, 24, 5)
