@@ -453,8 +453,9 @@ mr_status mr_trace_paths_static(const mr_scene* scene, const mr_integrator_setti
  * linear RGB, row-major, origin top-left (include/minirender/core/image.hpp). Host buffer.
  * A frame renders in waves of at most 8,388,608 paths (pixels x samples); a frame of several
  * waves sends them round several pooled path-state workspaces (about 2 GB each at full size),
- * each with its own stream, so that one wave's last bounces overlap the next waves' first. The
- * same holds for mr_render_device and mr_render_rows. */
+ * each with its own stream, so that one wave's last bounces overlap the next waves' first (a
+ * workspace that does not fit in device memory is left out; the image is the same). The same
+ * holds for mr_render_device and mr_render_rows. */
 mr_status mr_render(const mr_scene* scene, const mr_integrator_settings* integrator,
                     const mr_render_settings* render, float* rgb, mr_path_statistics* statistics);
 

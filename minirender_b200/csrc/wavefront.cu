@@ -1464,7 +1464,17 @@ void render_frame(const Scene& scene, const IntegratorParams& params, const mr_r
     if (total > capacity && max_paths == 0) {
         const size_t waves = (total + capacity - 1) / capacity;
         for (uint32_t i = 0; i + 1 < kFrameLanes && i + 1 < waves; ++i) {
-            more.ws[i]       = acquire_workspace(capacity, params.maximum_depth + 1, 0);
+            // A lane that does not fit in device memory is left out: the frame renders on the
+            // lanes it has (the same image, less overlap).
+            try {
+                more.ws[i] = acquire_workspace(capacity, params.maximum_depth + 1, 0);
+            } catch (const Error& e) {
+                if (e.status != MR_OUT_OF_MEMORY) {
+                    throw;
+                }
+                (void)cudaGetLastError();  // a failed allocation is not a sticky error
+                break;
+            }
             more.lanes[i].ws = more.ws[i].get();
             ++more.count;
             MR_CUDA(cudaStreamCreateWithFlags(&more.lanes[i].stream, cudaStreamNonBlocking));
