@@ -30,3 +30,19 @@ def test_reference_arm_prints_the_contract_line():
     assert line["config"] == bench.config(table)
     assert line["config"]["triangles_total"] == sum(
         sc.job_scene_triangles(j["triangles"]) for j in table)
+
+
+def test_quintile_bound_is_plain_time_over_time_at_the_best_batched_rate():
+    sys.path.insert(0, ROOT)
+    import bench
+    # Two fifths: 100 M samples at 200 plain / 300 batched, 900 M samples at 400 / 390.
+    quintiles = [{"samples": 100e6, "plain": 200.0, "batched": 300.0},
+                 {"samples": 900e6, "plain": 400.0, "batched": 390.0}]
+    bound = bench.quintile_bound(quintiles)
+    plain_s = 100e6 / 200.0 + 900e6 / 400.0
+    ideal_s = 1000e6 / 390.0
+    assert abs(bound["value"] - plain_s / ideal_s) < 1e-12 and bound["full_gpu_rate"] == 390.0
+    # A mix whose batched rates never beat the plain ones is bounded by the best of them.
+    flat = [{"samples": 1e6, "plain": 100.0, "batched": 100.0}] * 5
+    assert abs(bench.quintile_bound(flat)["value"] - 1.0) < 1e-12
+    assert bench.quintile_bound([]) is None
