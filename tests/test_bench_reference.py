@@ -1,5 +1,6 @@
-"""bench.py's reference arm (the CPU oracle on the host cores) prints one JSON line with the
-contract's keys; run on a small budget here."""
+"""bench.py on the CPU: the reference arm (the CPU oracle on the host cores) prints one JSON line
+with the contract's keys, run on a small budget here; the batched/plain bound the GPU arm reports
+is the plain path's time over the time at the best batched rate of any fifth of the mix."""
 
 import json
 import os
