@@ -2,9 +2,8 @@
 
 ``write_exr`` follows Image::write_exr (src/core/exr_io.cpp:36-110): three 32-bit float channels
 named B, G, R (sorted by name, as OpenEXR requires), linear values, nonfinite values rejected. The
-reference encodes with tinyexr using ZIP compression; this writer stores the scanlines
-uncompressed (compression NONE), which every OpenEXR reader accepts and which carries the same
-pixels. ``write_png`` follows Image::write_png (src/core/raster_io.cpp:115-138): 8-bit RGB, each
+reference encodes with tinyexr using ZIP compression (blocks of 16 scanlines, deflated after
+OpenEXR's byte split and delta predictor), and so does this writer. ``write_png`` follows Image::write_png (src/core/raster_io.cpp:115-138): 8-bit RGB, each
 channel through linear_to_srgb and a rounded unorm8 encoding (src/core/image.cpp:26-47); the
 reference encodes with stb_image_write, this writer with zlib (filter 0 per row).
 """
@@ -58,9 +57,21 @@ def _attribute(name: str, kind: str, value: bytes) -> bytes:
     return name.encode() + b"\x00" + kind.encode() + b"\x00" + struct.pack("<i", len(value)) + value
 
 
+def _zip_block(raw: bytes) -> bytes:
+    """OpenEXR's ZIP coding of one block: the bytes split into even- and odd-indexed halves, each
+    byte replaced by its difference from the previous one plus 128 (mod 256), then deflated. A
+    block that does not shrink is stored as it is, as the format prescribes."""
+    b = np.frombuffer(raw, np.uint8)
+    t = np.concatenate([b[0::2], b[1::2]]).astype(np.int16)
+    d = t.copy()
+    d[1:] = (t[1:] - t[:-1] + 128) & 0xFF
+    packed = zlib.compress(d.astype(np.uint8).tobytes(), 6)
+    return packed if len(packed) < len(raw) else raw
+
+
 def write_exr(path: str, rgb: np.ndarray):
-    """Scanline OpenEXR of a linear (height, width, 3) image: FLOAT channels B, G, R, no
-    compression, increasing-Y line order, one scanline per block."""
+    """Scanline OpenEXR of a linear (height, width, 3) image: FLOAT channels B, G, R, ZIP
+    compression (blocks of 16 scanlines), increasing-Y line order."""
     rgb = np.asarray(rgb, F32)
     height, width = rgb.shape[:2]
     if width == 0 or height == 0 or width * height > 2 ** 31 - 1:
@@ -72,7 +83,7 @@ def write_exr(path: str, rgb: np.ndarray):
     box = struct.pack("<iiii", 0, 0, width - 1, height - 1)
     header = (struct.pack("<ii", 20000630, 2)
               + _attribute("channels", "chlist", channels)
-              + _attribute("compression", "compression", b"\x00")
+              + _attribute("compression", "compression", b"\x03")
               + _attribute("dataWindow", "box2i", box)
               + _attribute("displayWindow", "box2i", box)
               + _attribute("lineOrder", "lineOrder", b"\x00")
@@ -80,17 +91,19 @@ def write_exr(path: str, rgb: np.ndarray):
               + _attribute("screenWindowCenter", "v2f", struct.pack("<ff", 0.0, 0.0))
               + _attribute("screenWindowWidth", "float", struct.pack("<f", 1.0))
               + b"\x00")
-    line_bytes = width * 3 * 4
-    block = 8 + line_bytes
-    first = len(header) + 8 * height
-    offsets = struct.pack(f"<{height}Q", *(first + y * block for y in range(height)))
+    lines = 16
     planes = np.ascontiguousarray(rgb[:, :, ::-1].transpose(0, 2, 1), dtype="<f4")  # B, G, R
+    blocks = [_zip_block(planes[y:y + lines].tobytes()) for y in range(0, height, lines)]
+    offsets, at = [], len(header) + 8 * len(blocks)
+    for block in blocks:
+        offsets.append(at)
+        at += 8 + len(block)
     with open(path, "wb") as f:
         f.write(header)
-        f.write(offsets)
-        for y in range(height):
-            f.write(struct.pack("<ii", y, line_bytes))
-            f.write(planes[y].tobytes())
+        f.write(struct.pack(f"<{len(blocks)}Q", *offsets))
+        for k, block in enumerate(blocks):
+            f.write(struct.pack("<ii", k * lines, len(block)))
+            f.write(block)
 
 
 # ---- texture input (Image::read, src/core/raster_io.cpp:40-113) ----
